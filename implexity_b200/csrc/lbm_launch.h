@@ -1,0 +1,120 @@
+// lbm_launch.h -- host-side launchers of the sm_100a kernels (lbm_kernels.cu).
+// Every launcher enqueues on the given stream and returns the launch status.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "lbm_common.cuh"
+
+namespace lbm {
+
+// Population storage.  F32 stores g = f - w; F16/BF16 store g/w.
+enum StoreKind { ST_F32 = 0, ST_F16 = 1, ST_BF16 = 2 };
+enum CollKind { CK_PAIRS = 0, CK_MRT = 1 };  // BGK runs as PAIRS with om == omega
+
+struct FwdArgs {
+    Geometry G;
+    Physics P;
+    void* pop;               // Q planes of n cells (storage type)
+    const uint32_t* mask;
+    const float* alpha;
+    const PortMap* ports;
+    int32_t parity;          // 0: in-place swap step, 1: neighbour step
+    int32_t apply_ports;     // the stored state still needs the port reconstruction
+    StepDiag* diag;          // per-state admission output (nullptr: off)
+    Reduce red;
+    float* record;           // (rho-1, ux, uy, uz) planes (nullptr: off)
+    int32_t collide;         // 0: only load/diag/record (no collision, no store)
+};
+
+struct AdjArgs {
+    Geometry G;
+    Physics P;
+    void* lam;               // Q planes of n cells (lambda storage type)
+    const uint32_t* mask;
+    const float* alpha;
+    const PortMap* ports;
+    const float* record;     // (rho-1, ux, uy, uz) of the forward state
+    float* abar;             // accumulated alpha cotangent
+    int32_t parity;
+    int32_t port_transpose;  // store Ports^T lambda (1) or lambda itself (0)
+    int32_t overwrite_abar;  // abar = (1) or += (0)
+    float in_scale_inv;      // true = stored * in_scale_inv
+    float out_scale;         // stored = true * out_scale
+    float abar_factor;       // abar += factor * d(loss)/d(alpha)
+    double* norm2;           // sum of squares of the stored lambda (true units * out_scale), nullptr: off
+    Reduce red;
+};
+
+struct ObjArgs {
+    Geometry G;
+    Physics P;
+    const void* pop;
+    const uint32_t* mask;
+    const float* alpha;
+    const float* phi;
+    const PortMap* ports;
+    int32_t parity;
+    int32_t apply_ports;
+    float tau;
+    // response scales
+    float vel, dens, dt_s;
+    double w[8];             // weights after the reference's scalings (seed only)
+    // outputs
+    double* sums;            // responses: 16 doubles (8 compensated pairs)
+    Reduce red;
+    float* fields;           // optional (rho-1, ux, uy, uz) planes
+    // seed outputs
+    void* lam;
+    float lam_scale;
+    float* abar_final;
+    float* phibar;
+    float* record;
+    double* norm2;
+    int32_t write_lambda;
+    int32_t port_transpose;
+};
+
+struct DesignArgs {
+    Geometry G;
+    const float* raw;
+    const uint8_t* cls;      // 0 solid, 1 editable, 2 fixed
+    const float* fixed;
+    const int4* offsets;     // (dx, dy, dz, float-bits weight)
+    int32_t n_offsets;
+    float beta, eta, proj_a, proj_den;
+    float ramp_c, ramp_q;    // alpha = c (1-phi)/(q+phi), c = dt*drag_max*q
+    float* phi;
+    float* alpha;
+    float* den;
+    float* slope;
+    // sensitivity
+    const float* phibar;
+    const float* abar;
+    const float* abar_final;
+    float abar_scale;
+    float* scale;
+    float* grad;
+};
+
+cudaError_t launch_init(int Q, int storage, const Geometry& G, const Physics& P, void* pop, const uint32_t* mask,
+                        cudaStream_t s);
+cudaError_t launch_forward(int Q, int coll, int storage, const FwdArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_adjoint(int Q, int coll, int lstorage, const AdjArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_objective(int Q, int storage, int lstorage, int mode, const ObjArgs& a, int grid,
+                             cudaStream_t s);  // mode 0: responses/fields, 1: seed
+cudaError_t launch_canon_pop(int Q, int storage, const Geometry& G, const void* pop, const uint32_t* mask,
+                             const PortMap* ports, int parity, int apply_ports, float* out, int grid,
+                             cudaStream_t s);
+cudaError_t launch_upload_pop(int Q, int storage, const Geometry& G, void* pop, const float* in, int grid,
+                              cudaStream_t s);
+cudaError_t launch_canon_lam(int Q, int lstorage, const Geometry& G, const void* lam, const uint32_t* mask,
+                             int after_odd, float inv_scale, float* out, int grid, cudaStream_t s);
+cudaError_t launch_seed_lam(int Q, int lstorage, const Geometry& G, void* lam, const uint32_t* mask,
+                            const PortMap* ports, const float* in, float scale, int port_transpose, int grid,
+                            cudaStream_t s);
+cudaError_t launch_design_map(const DesignArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_sens_scale(const DesignArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_filter_transpose(const DesignArgs& a, int grid, cudaStream_t s);
+
+}  // namespace lbm

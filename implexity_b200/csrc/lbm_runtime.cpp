@@ -1,0 +1,1439 @@
+// lbm_runtime.cpp -- host runtime behind the C-ABI of include/lbm_b200.h:
+// problem validation and normalisation (with the reference's contract
+// messages), link masks, port maps and design filter, device memory, the
+// forward / adjoint schedules and the admission record.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <charconv>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/lbm_b200.h"
+#include "lbm_common.cuh"
+#include "lbm_launch.h"
+
+using namespace lbm;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct ContractError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct StateError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct ConvergenceError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+#define CK(expr)                                                                                   \
+    do {                                                                                           \
+        cudaError_t _e = (expr);                                                                   \
+        if (_e != cudaSuccess)                                                                     \
+            throw CudaError(std::string(#expr) + ": " + cudaGetErrorString(_e));                   \
+    } while (0)
+
+// Python-style shortest float repr (implexity_core::py_repr::repr_float).
+std::string repr_float(double v) {
+    if (std::isnan(v)) return "nan";
+    if (std::isinf(v)) return v > 0 ? "inf" : "-inf";
+    char buf[64];
+    auto r = std::to_chars(buf, buf + sizeof(buf), v, std::chars_format::scientific);
+    std::string sci(buf, r.ptr);
+    // split mantissa digits and exponent
+    size_t epos = sci.find('e');
+    std::string mant = sci.substr(0, epos);
+    int exp10 = std::stoi(sci.substr(epos + 1));
+    bool neg = !mant.empty() && mant[0] == '-';
+    if (neg) mant = mant.substr(1);
+    std::string digits;
+    for (char c : mant)
+        if (c != '.') digits += c;
+    std::string out;
+    if (exp10 >= -5 && exp10 < 16) {
+        if (exp10 >= 0) {
+            if ((int)digits.size() <= exp10 + 1) out = digits + std::string(exp10 + 1 - digits.size(), '0') + ".0";
+            else out = digits.substr(0, exp10 + 1) + "." + digits.substr(exp10 + 1);
+        } else {
+            out = "0." + std::string(-exp10 - 1, '0') + digits;
+        }
+    } else {
+        out = digits.substr(0, 1);
+        if (digits.size() > 1) out += "." + digits.substr(1);
+        char e[16];
+        std::snprintf(e, sizeof(e), "e%c%02d", exp10 < 0 ? '-' : '+', std::abs(exp10));
+        out += e;
+    }
+    return neg ? "-" + out : out;
+}
+
+// ------------------------------------------------------------ lattice (host)
+struct HostLat {
+    int Q;
+    int c[27][3];
+    double w[27];
+    int opp[27];
+};
+template <int Q>
+HostLat host_lat_t() {
+    HostLat L;
+    L.Q = Q;
+    for (int q = 0; q < Q; ++q) {
+        L.c[q][0] = Lat<Q>::cx(q);
+        L.c[q][1] = Lat<Q>::cy(q);
+        L.c[q][2] = Lat<Q>::cz(q);
+        L.w[q] = Lat<Q>::wd(q);
+        L.opp[q] = opp<Q>(q);
+    }
+    return L;
+}
+HostLat host_lat(int Q) { return Q == 19 ? host_lat_t<19>() : host_lat_t<27>(); }
+
+// Gram-Schmidt moment basis (moving/collision.rs:87-153): candidate
+// polynomials mass, momentum, bulk |c|^2, shear, then the monomials of
+// degree 3..6 with exponents <= 2, orthogonalised in the w-weighted inner
+// product.  Returns rows/norms/groups (0 mass 1 momentum 2 bulk 3 shear
+// 4 odd 5 even-high) or false if the basis is incomplete.
+bool moment_basis(const HostLat& L, std::vector<std::vector<double>>& rows, std::vector<double>& norms,
+                  std::vector<int>& groups) {
+    const int Q = L.Q;
+    std::vector<std::pair<std::vector<double>, int>> cand;
+    auto add = [&](auto fn, int g) {
+        std::vector<double> p(Q);
+        for (int i = 0; i < Q; ++i) p[i] = fn(L.c[i][0], L.c[i][1], L.c[i][2]);
+        cand.push_back({p, g});
+    };
+    add([](int, int, int) { return 1.0; }, 0);
+    add([](int x, int, int) { return (double)x; }, 1);
+    add([](int, int y, int) { return (double)y; }, 1);
+    add([](int, int, int z) { return (double)z; }, 1);
+    add([](int x, int y, int z) { return (double)(x * x + y * y + z * z); }, 2);
+    add([](int x, int y, int z) { return (double)(2 * x * x - y * y - z * z); }, 3);
+    add([](int, int y, int z) { return (double)(y * y - z * z); }, 3);
+    add([](int x, int y, int) { return (double)(x * y); }, 3);
+    add([](int x, int, int z) { return (double)(x * z); }, 3);
+    add([](int, int y, int z) { return (double)(y * z); }, 3);
+    for (int deg = 3; deg <= 6; ++deg)
+        for (int a = 0; a <= 2; ++a)
+            for (int b = 0; b <= 2; ++b) {
+                int c = deg - a - b;
+                if (c < 0 || c > 2) continue;
+                add([=](int x, int y, int z) { return std::pow(x, a) * std::pow(y, b) * std::pow(z, c); },
+                    deg % 2 ? 4 : 5);
+            }
+    auto inner = [&](const std::vector<double>& x, const std::vector<double>& y) {
+        double s = 0;
+        for (int i = 0; i < Q; ++i) s += L.w[i] * x[i] * y[i];
+        return s;
+    };
+    rows.clear();
+    norms.clear();
+    groups.clear();
+    for (auto& [p, g] : cand) {
+        if ((int)rows.size() == Q) break;
+        double scale = inner(p, p);
+        if (scale <= 0) continue;
+        std::vector<double> v = p;
+        for (size_t k = 0; k < rows.size(); ++k) {
+            double coef = inner(p, rows[k]) / norms[k];
+            for (int i = 0; i < Q; ++i) v[i] -= coef * rows[k][i];
+        }
+        double n = inner(v, v);
+        if (n <= 1e-10 * scale) continue;
+        rows.push_back(v);
+        norms.push_back(n);
+        groups.push_back(g);
+    }
+    return (int)rows.size() == Q;
+}
+
+// Legacy-moment port reconstruction (ports.rs:343-406) in FP64, used once
+// per port to tabulate its affine map.
+struct PortSpec {
+    bool pressure;
+    int axis, sign;
+    double vel[3];
+    double density;
+};
+
+void reconstruct(const HostLat& L, const PortSpec& p, const double a[3], const double* f, double* out) {
+    const int Q = L.Q;
+    std::vector<int> unknown;
+    double compat = 0, out_sum = 0;
+    for (int q = 0; q < Q; ++q) {
+        if (L.c[q][p.axis] == p.sign) unknown.push_back(q);
+        else if (L.c[q][p.axis] == -p.sign) out_sum += f[q];
+        else compat += f[q];
+    }
+    compat += 2.0 * out_sum;
+    int t[2], nt = 0;
+    for (int d = 0; d < 3; ++d)
+        if (d != p.axis) t[nt++] = d;
+    double v[3];
+    for (int d = 0; d < 3; ++d) v[d] = p.vel[d] - 0.5 * a[d];
+    double rho;
+    if (!p.pressure) rho = compat / (1.0 - p.sign * v[p.axis]);
+    else {
+        rho = p.density;
+        v[p.axis] = (1.0 - compat / rho) * p.sign;
+    }
+    const int U = (int)unknown.size();
+    std::vector<double> prop(U);
+    for (int k = 0; k < U; ++k) {
+        int q = unknown[k];
+        double cv = L.c[q][0] * v[0] + L.c[q][1] * v[1] + L.c[q][2] * v[2];
+        prop[k] = f[L.opp[q]] + rho * 6.0 * L.w[q] * cv;
+    }
+    double km = 0, kj[3] = {0, 0, 0};
+    for (int q = 0; q < Q; ++q) {
+        if (L.c[q][p.axis] == p.sign) continue;
+        km += f[q];
+        for (int d = 0; d < 3; ++d) kj[d] += f[q] * L.c[q][d];
+    }
+    double target[3] = {rho - km, rho * v[t[0]] - kj[t[0]], rho * v[t[1]] - kj[t[1]]};
+    double pa[3] = {0, 0, 0};
+    double R[3][9];
+    for (int k = 0; k < U; ++k) {
+        int q = unknown[k];
+        R[0][k] = 1.0;
+        R[1][k] = L.c[q][t[0]];
+        R[2][k] = L.c[q][t[1]];
+        for (int r = 0; r < 3; ++r) pa[r] += prop[k] * R[r][k];
+    }
+    double res[3] = {target[0] - pa[0], target[1] - pa[1], target[2] - pa[2]};
+    double M[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double s = 0;
+            for (int k = 0; k < U; ++k) s += R[i][k] * R[j][k];
+            M[i][j] = s;
+        }
+    // 3x3 inverse by cofactors
+    double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                 M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+    double inv[3][3] = {};
+    if (det != 0.0) {
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                int i1 = (j + 1) % 3, i2 = (j + 2) % 3, j1 = (i + 1) % 3, j2 = (i + 2) % 3;
+                inv[i][j] = (M[i1][j1] * M[i2][j2] - M[i1][j2] * M[i2][j1]) / det;
+            }
+    }
+    for (int q = 0; q < Q; ++q) out[q] = f[q];
+    for (int k = 0; k < U; ++k) {
+        double corr = 0;
+        for (int j = 0; j < 3; ++j) {
+            double rij = R[0][k] * inv[0][j] + R[1][k] * inv[1][j] + R[2][k] * inv[2][j];
+            corr += res[j] * rij;
+        }
+        out[unknown[k]] = prop[k] + corr;
+    }
+}
+
+// ------------------------------------------------------------ device buffers
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int64_t* counter = nullptr;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { reset(); }
+    void reset() {
+        if (p) {
+            cudaFree(p);
+            if (counter) *counter -= (int64_t)bytes;
+        }
+        p = nullptr;
+        bytes = 0;
+    }
+    void alloc(size_t b, int64_t* ctr) {
+        if (p && bytes >= b) return;
+        reset();
+        counter = ctr;
+        CK(cudaMalloc(&p, b));
+        bytes = b;
+        if (counter) *counter += (int64_t)b;
+    }
+    template <typename T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
+size_t storage_bytes(int s) { return s == LBM_STORE_F32 ? 4 : 2; }
+
+}  // namespace
+
+struct Checkpoint {
+    std::unique_ptr<DevBuf> buf;
+    int64_t t;
+    int parity;
+    bool pending;
+};
+
+struct lbm_handle {
+    // --- normalised problem
+    int Q = 19, coll = LBM_BGK, storage = LBM_STORE_F32;
+    Geometry G{};
+    Physics P{};
+    HostLat L{};
+    double tau = 0, omega = 0, om = 0;
+    double a[3] = {0, 0, 0};
+    int64_t step_count = 0;
+    double dx = 0, dt = 0, density = 0, mach_limit = 0, drag_max = 0, drag_shape = 0;
+    int64_t fluid_cells = 0, n_inlet = 0, n_outlet = 0;
+    int n_ports = 0;
+    std::vector<uint8_t> cls;
+    std::vector<int4> offsets;
+    float beta = 0, eta = 0.5f, proj_a = 0, proj_den = 1;
+    // --- device
+    int device = 0, sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int64_t device_bytes = 0;
+    DevBuf pop, mask, alpha, phi, raw, den, slope, cls_d, fixed_d, offsets_d, ports_d, partial, counter, diag;
+    DevBuf lam, record, abar, abar_final, phibar, scale, grad, norm2, sums, scratch;
+    int lam_storage = LBM_STORE_F32;
+    std::vector<Checkpoint> ckpts;
+    // --- state
+    bool design_set = false, state_valid = false, forward_done = false;
+    int parity = 0;
+    bool pending = false;
+    int64_t t = 0;
+    std::string err;
+
+    int64_t n() const { return G.n; }
+};
+
+namespace {
+
+// ------------------------------------------------------------ validation
+void require(bool ok, const char* msg) {
+    if (!ok) throw ContractError(msg);
+}
+bool finite_positive(double v) { return std::isfinite(v) && v > 0; }
+
+void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
+    // solver.rs:414-550 in order; key-set and array-shape checks belong to the
+    // JSON layer of the caller.
+    require(p.lattice == 19 || p.lattice == 27, "lattice must be D3Q19 or D3Q27");
+    require(p.collision >= LBM_BGK && p.collision <= LBM_MRT, "collision must be bgk, trt or mrt");
+    require(p.storage >= LBM_STORE_F32 && p.storage <= LBM_STORE_BF16, "storage must be float32, float16 or bfloat16");
+    require(p.shape[0] >= 2 && p.shape[1] >= 2 && p.shape[2] >= 2, "LBM shape must contain three integers >= 2");
+    const char* names[7] = {"spacing_m", "step_s", "density_kg_m3", "kinematic_viscosity_m2_s", "drag_max_per_s",
+                            "drag_shape", "mach_limit"};
+    double vals[7] = {p.spacing_m,      p.step_s,     p.density_kg_m3, p.kinematic_viscosity_m2_s,
+                      p.drag_max_per_s, p.drag_shape, p.mach_limit};
+    for (int i = 0; i < 7; ++i)
+        if (!finite_positive(vals[i])) throw ContractError(std::string(names[i]) + " must be a finite positive scalar");
+    require(p.mach_limit <= 0.2, "LBM mach_limit must be <= 0.2; this is not a compressible gas solver");
+    require(p.step_count >= 1 && p.step_count <= 1000000, "step_count must be an integer in [1,1000000]");
+    const int64_t n = (int64_t)p.shape[0] * p.shape[1] * p.shape[2];
+    require(p.solid_mask && p.design_region && p.fixed_design, "solid_mask must be a shape-matched boolean array");
+    for (int64_t x = 0; x < n; ++x) {
+        double v = p.fixed_design[x];
+        require(std::isfinite(v) && v >= 0.0 && v <= 1.0, "fixed_design must be finite and in [0,1]");
+    }
+    bool all_solid = true, overlap = false;
+    for (int64_t x = 0; x < n; ++x) {
+        all_solid = all_solid && p.solid_mask[x];
+        overlap = overlap || (p.solid_mask[x] && p.design_region[x]);
+    }
+    require(!all_solid && !overlap, "Need fluid cells; fixed solid cells cannot be designable");
+    for (int d = 0; d < 3; ++d)
+        require(std::isfinite(p.acceleration_m_s2[d]), "acceleration_m_s2 requires three finite components");
+    double tau = 0.5 + 3.0 * p.kinematic_viscosity_m2_s * p.step_s / (p.spacing_m * p.spacing_m);
+    require(tau >= 0.51 && tau <= 2.0, "Choose spacing/time step such that 0.51 <= relaxation time <= 2");
+    // topology map, design.rs:52-83
+    require(std::isfinite(p.filter_radius_m) && std::isfinite(p.projection_beta) && std::isfinite(p.projection_eta),
+            "topology_map.filter_radius_m must be finite real scalar");
+    require(p.filter_radius_m >= 0.0 && p.filter_radius_m <= 4.0 * p.spacing_m,
+            "filter_radius_m must lie in [0,4*spacing_m]");
+    require(p.projection_beta >= 0.0 && p.projection_beta <= 32.0 && p.projection_eta > 0.0 && p.projection_eta < 1.0,
+            "Require beta in [0,32] and eta in (0,1)");
+    require(p.filter_kind == LBM_FILTER_CONIC || p.filter_kind == LBM_FILTER_BOX, "filter_kind must be conic or box");
+    require(p.filter_kind != LBM_FILTER_BOX || (p.box_half_width >= 0 && p.box_half_width <= 4),
+            "box filter half width must lie in [0,4] cells");
+    // collision parameters, moving/collision.rs:236-256
+    if (p.collision == LBM_TRT) {
+        double m = std::isnan(p.trt_magic) ? 3.0 / 16.0 : p.trt_magic;
+        require(std::isfinite(m) && m > 0, "TRT magic parameter must be finite and positive");
+    }
+    if (p.collision == LBM_MRT) {
+        double m = std::isnan(p.mrt_odd_magic) ? 3.0 / 16.0 : p.mrt_odd_magic;
+        require(std::isfinite(m) && m > 0, "MRT odd_magic must be finite and positive");
+        auto ok = [](double r) { return std::isnan(r) || (std::isfinite(r) && r > 0 && r < 2); };
+        require(ok(p.mrt_bulk_rate) && ok(p.mrt_even_rate), "MRT relaxation rates must lie in (0, 2)");
+    }
+
+    h.Q = p.lattice;
+    h.coll = p.collision;
+    h.storage = p.storage;
+    h.L = host_lat(h.Q);
+    h.G.n = n;
+    h.G.nx = p.shape[0];
+    h.G.ny = p.shape[1];
+    h.G.nz = p.shape[2];
+    h.G.periodic = (p.periodic_axes[0] ? 1 : 0) | (p.periodic_axes[1] ? 2 : 0) | (p.periodic_axes[2] ? 4 : 0);
+    h.G.sx = (int64_t)p.shape[1] * p.shape[2];
+    h.G.sy = p.shape[2];
+    h.tau = tau;
+    h.dx = p.spacing_m;
+    h.dt = p.step_s;
+    h.density = p.density_kg_m3;
+    h.mach_limit = p.mach_limit;
+    h.drag_max = p.drag_max_per_s;
+    h.drag_shape = p.drag_shape;
+    h.step_count = p.step_count;
+    for (int d = 0; d < 3; ++d) h.a[d] = p.acceleration_m_s2[d] * p.step_s * p.step_s / p.spacing_m;
+    h.omega = 1.0 / tau;
+    double magic = p.collision == LBM_MRT ? p.mrt_odd_magic : p.trt_magic;
+    if (std::isnan(magic)) magic = 3.0 / 16.0;
+    h.om = p.collision == LBM_BGK ? h.omega : 1.0 / (0.5 + magic / (tau - 0.5));
+    h.P.omega = (float)h.omega;
+    h.P.om = (float)h.om;
+    for (int d = 0; d < 3; ++d) h.P.a[d] = (float)h.a[d];
+    h.P.n_proj = 0;
+    if (p.collision == LBM_MRT) {
+        std::vector<std::vector<double>> rows;
+        std::vector<double> norms;
+        std::vector<int> groups;
+        require(moment_basis(h.L, rows, norms, groups), "MRT moment basis is incomplete");
+        for (int k = 0; k < h.Q; ++k) {
+            double rate;
+            if (groups[k] == 2) rate = std::isnan(p.mrt_bulk_rate) ? h.omega : p.mrt_bulk_rate;
+            else if (groups[k] == 5) rate = std::isnan(p.mrt_even_rate) ? h.omega : p.mrt_even_rate;
+            else continue;
+            if (rate == h.omega) continue;
+            int j = h.P.n_proj++;
+            h.P.proj_rate[j] = (float)(rate - h.omega);
+            for (int i = 0; i < h.Q; ++i) {
+                h.P.proj_left[j][i] = (float)(h.L.w[i] * rows[k][i] / norms[k]);
+                h.P.proj_right[j][i] = (float)rows[k][i];
+            }
+        }
+    }
+
+    // ports (ports.rs:106-272)
+    require(p.n_ports >= 0 && (p.n_ports == 0 || p.ports), "ports must be a list");
+    require(p.n_ports <= LBM_MAX_PORTS, "at most 7 ports are supported");
+    std::vector<uint8_t> used(n, 0);
+    std::vector<PortSpec> specs;
+    std::vector<std::vector<int64_t>> port_cells;
+    const bool periodic[3] = {p.periodic_axes[0] != 0, p.periodic_axes[1] != 0, p.periodic_axes[2] != 0};
+    const int64_t shape[3] = {p.shape[0], p.shape[1], p.shape[2]};
+    for (int k = 0; k < p.n_ports; ++k) {
+        const lbm_port_t& pt = p.ports[k];
+        require(pt.kind == LBM_PORT_VELOCITY || pt.kind == LBM_PORT_PRESSURE, "Port kind must be velocity or pressure");
+        require(pt.face >= 0 && pt.face <= 5, "Port must identify one Cartesian face");
+        PortSpec s;
+        s.pressure = pt.kind == LBM_PORT_PRESSURE;
+        s.axis = pt.face / 2;
+        s.sign = pt.face % 2 == 0 ? 1 : -1;
+        require(!periodic[s.axis], "A periodic face cannot be a port");
+        bool any = false;
+        if (pt.mask)
+            for (int64_t x = 0; x < n; ++x) any = any || pt.mask[x];
+        require(any, "Nonempty shape-matched boolean port mask required");
+        const int64_t face_index = s.sign == 1 ? 0 : shape[s.axis] - 1;
+        std::vector<int64_t> cells;
+        for (int64_t x = 0; x < n; ++x) {
+            if (!pt.mask[x]) continue;
+            int64_t c[3] = {x / h.G.sx, (x / h.G.sy) % shape[1], x % shape[2]};
+            require(c[s.axis] == face_index && !used[x], "Port mask must lie on its face and cannot overlap another port");
+            cells.push_back(x);
+        }
+        for (int a2 = 0; a2 < 3; ++a2) {
+            if (a2 == s.axis || periodic[a2]) continue;
+            for (int64_t x : cells) {
+                int64_t c[3] = {x / h.G.sx, (x / h.G.sy) % shape[1], x % shape[2]};
+                require(!(c[a2] == 0 || c[a2] == shape[a2] - 1),
+                        "Port corners/edges with other closed faces require an unsupported corner closure");
+            }
+        }
+        for (int64_t x : cells)
+            require(!(p.solid_mask[x] || p.design_region[x] || p.fixed_design[x] != 1.0),
+                    "Port cells must be protected, unobstructed, fixed-design fluid");
+        for (int d = 0; d < 3; ++d)
+            require(std::isfinite(pt.velocity_m_s[d]), "Port velocity requires three finite components");
+        for (int d = 0; d < 3; ++d) s.vel[d] = pt.velocity_m_s[d] * p.step_s / p.spacing_m;
+        require(!(s.pressure && pt.velocity_m_s[s.axis] != 0.0),
+                "Pressure port velocity specifies tangential components only; normal component must be zero");
+        double un = std::sqrt(s.vel[0] * s.vel[0] + s.vel[1] * s.vel[1] + s.vel[2] * s.vel[2]);
+        require(!(un * std::sqrt(3.0) > p.mach_limit), "Authored port velocity exceeds Mach limit");
+        s.density = 1.0;
+        if (s.pressure) {
+            require(std::isfinite(pt.gauge_pressure_Pa), "Finite scalar gauge pressure required");
+            double unit = p.spacing_m / p.step_s;
+            double rho = 1.0 + pt.gauge_pressure_Pa * 3.0 / (p.density_kg_m3 * unit * unit);
+            require(rho >= 0.9 && rho <= 1.1, "Pressure port density must remain within 10% of reference");
+            s.density = rho;
+        }
+        for (int64_t x : cells) used[x] = 1;
+        specs.push_back(s);
+        port_cells.push_back(cells);
+    }
+    h.n_ports = (int)specs.size();
+    h.n_inlet = h.n_outlet = 0;
+    for (size_t k = 0; k < specs.size(); ++k) (specs[k].pressure ? h.n_outlet : h.n_inlet) += (int64_t)port_cells[k].size();
+
+    // port affine maps in shifted variables
+    std::vector<PortMap> maps(specs.size());
+    for (size_t k = 0; k < specs.size(); ++k) {
+        PortMap& M = maps[k];
+        std::memset(&M, 0, sizeof(M));
+        const int Q = h.Q;
+        double base[27], pert[27], r0[27], r1[27];
+        for (int q = 0; q < Q; ++q) base[q] = h.L.w[q];
+        reconstruct(h.L, specs[k], h.a, base, r0);
+        for (int q = 0; q < Q; ++q)
+            if (h.L.c[q][specs[k].axis] == specs[k].sign) M.unknown_mask |= 1u << q;
+        for (int r = 0; r < Q; ++r)
+            if (M.unknown_mask & (1u << r)) M.bias[r] = (float)(r0[r] - h.L.w[r]);
+        for (int kq = 0; kq < Q; ++kq) {
+            for (int q = 0; q < Q; ++q) pert[q] = base[q];
+            pert[kq] += 1.0;
+            reconstruct(h.L, specs[k], h.a, pert, r1);
+            for (int r = 0; r < Q; ++r)
+                if (M.unknown_mask & (1u << r)) M.jac[r][kq] = (float)(r1[r] - r0[r]);
+        }
+        bool both = h.n_inlet > 0 && h.n_outlet > 0;
+        M.dp_weight = !both ? 0.f : specs[k].pressure ? (float)(-1.0 / h.n_outlet) : (float)(1.0 / h.n_inlet);
+    }
+
+    // link masks (Streaming::new, solver.rs:84-119)
+    std::vector<uint32_t> mask(n, 0);
+    h.fluid_cells = 0;
+    for (int64_t x = 0; x < n; ++x) {
+        int64_t c[3] = {x / h.G.sx, (x / h.G.sy) % shape[1], x % shape[2]};
+        uint32_t m = 0;
+        if (p.solid_mask[x]) m |= MASK_SOLID;
+        else ++h.fluid_cells;
+        bool wraps = false;
+        for (int a2 = 0; a2 < 3; ++a2)
+            if (periodic[a2] && (c[a2] == 0 || c[a2] == shape[a2] - 1)) wraps = true;
+        if (wraps) m |= MASK_WRAP;
+        for (int q = 0; q < h.Q; ++q) {
+            int64_t s[3];
+            bool outside = false;
+            for (int a2 = 0; a2 < 3; ++a2) {
+                s[a2] = c[a2] - h.L.c[q][a2];
+                if (s[a2] < 0 || s[a2] >= shape[a2]) {
+                    if (!periodic[a2]) outside = true;
+                    s[a2] = (s[a2] % shape[a2] + shape[a2]) % shape[a2];
+                }
+            }
+            int64_t src = (s[0] * shape[1] + s[1]) * shape[2] + s[2];
+            if (outside || p.solid_mask[src]) m |= 1u << q;
+        }
+        mask[x] = m;
+    }
+    for (size_t k = 0; k < port_cells.size(); ++k)
+        for (int64_t x : port_cells[k]) mask[x] |= (uint32_t)(k + 1) << MASK_PORT_SHIFT;
+
+    // design map (design.rs:109-171); box filter is the documented extension
+    h.cls.assign(n, 0);
+    std::vector<float> fixed(n);
+    for (int64_t x = 0; x < n; ++x) {
+        h.cls[x] = p.solid_mask[x] ? 0 : (p.design_region[x] ? 1 : 2);
+        fixed[x] = (float)p.fixed_design[x];
+    }
+    h.offsets.clear();
+    if (p.filter_kind == LBM_FILTER_BOX) {
+        int hw = p.box_half_width;
+        if (hw > 0)
+            for (int i = -hw; i <= hw; ++i)
+                for (int j = -hw; j <= hw; ++j)
+                    for (int k = -hw; k <= hw; ++k) {
+                        float w = 1.f;
+                        int wb;
+                        std::memcpy(&wb, &w, 4);
+                        h.offsets.push_back(make_int4(i, j, k, wb));
+                    }
+    } else {
+        double radius = p.filter_radius_m / p.spacing_m;
+        if (radius > 0) {
+            int reach = (int)std::ceil(radius);
+            for (int i = -reach; i <= reach; ++i)
+                for (int j = -reach; j <= reach; ++j)
+                    for (int k = -reach; k <= reach; ++k) {
+                        double wgt = std::max(radius - std::sqrt((double)(i * i + j * j + k * k)), 0.0);
+                        if (wgt == 0.0) continue;
+                        float w = (float)wgt;
+                        int wb;
+                        std::memcpy(&wb, &w, 4);
+                        h.offsets.push_back(make_int4(i, j, k, wb));
+                    }
+        }
+    }
+    h.beta = (float)p.projection_beta;
+    h.eta = (float)p.projection_eta;
+    if (p.projection_beta > 0) {
+        double pa = std::tanh(p.projection_beta * p.projection_eta);
+        h.proj_a = (float)pa;
+        h.proj_den = (float)(pa + std::tanh(p.projection_beta * (1.0 - p.projection_eta)));
+    }
+
+    // --- device
+    CK(cudaGetDevice(&h.device));
+    CK(cudaDeviceGetAttribute(&h.sms, cudaDevAttrMultiProcessorCount, h.device));
+    CK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&h.ev0));
+    CK(cudaEventCreate(&h.ev1));
+    int64_t* ctr = &h.device_bytes;
+    h.pop.alloc((size_t)n * h.Q * storage_bytes(h.storage), ctr);
+    h.mask.alloc((size_t)n * 4, ctr);
+    h.alpha.alloc((size_t)n * 4, ctr);
+    h.phi.alloc((size_t)n * 4, ctr);
+    h.raw.alloc((size_t)n * 4, ctr);
+    h.den.alloc((size_t)n * 4, ctr);
+    h.slope.alloc((size_t)n * 4, ctr);
+    h.cls_d.alloc((size_t)n, ctr);
+    h.fixed_d.alloc((size_t)n * 4, ctr);
+    h.offsets_d.alloc(std::max<size_t>(1, h.offsets.size()) * sizeof(int4), ctr);
+    h.ports_d.alloc(std::max<size_t>(1, maps.size()) * sizeof(PortMap), ctr);
+    h.partial.alloc((size_t)h.sms * 32 * 16 * sizeof(double), ctr);
+    h.counter.alloc(sizeof(unsigned), ctr);
+    h.sums.alloc(64 * sizeof(double), ctr);
+    CK(cudaMemcpyAsync(h.mask.p, mask.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h.stream));
+    CK(cudaMemcpyAsync(h.cls_d.p, h.cls.data(), (size_t)n, cudaMemcpyHostToDevice, h.stream));
+    CK(cudaMemcpyAsync(h.fixed_d.p, fixed.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h.stream));
+    if (!h.offsets.empty())
+        CK(cudaMemcpyAsync(h.offsets_d.p, h.offsets.data(), h.offsets.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                           h.stream));
+    if (!maps.empty())
+        CK(cudaMemcpyAsync(h.ports_d.p, maps.data(), maps.size() * sizeof(PortMap), cudaMemcpyHostToDevice,
+                           h.stream));
+    CK(cudaMemsetAsync(h.counter.p, 0, sizeof(unsigned), h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+}
+
+// ------------------------------------------------------------ stepping
+int grid_for(const lbm_handle& h) {
+    int64_t b = (h.n() + 255) / 256;
+    int64_t cap = (int64_t)h.sms * 8;
+    return (int)std::max<int64_t>(1, std::min(b, cap));
+}
+
+Reduce reduce_of(lbm_handle& h) { return Reduce{h.partial.as<double>(), h.counter.as<unsigned>()}; }
+
+FwdArgs fwd_args(lbm_handle& h) {
+    FwdArgs a{};
+    a.G = h.G;
+    a.P = h.P;
+    a.pop = h.pop.p;
+    a.mask = h.mask.as<uint32_t>();
+    a.alpha = h.alpha.as<float>();
+    a.ports = h.ports_d.as<PortMap>();
+    a.red = reduce_of(h);
+    return a;
+}
+
+int coll_kind(const lbm_handle& h) { return h.coll == LBM_MRT ? CK_MRT : CK_PAIRS; }
+
+// One step of the current state; diag / record optional.
+void step(lbm_handle& h, StepDiag* diag, float* record) {
+    FwdArgs a = fwd_args(h);
+    a.parity = h.parity;
+    a.apply_ports = h.pending ? 1 : 0;
+    a.diag = diag;
+    a.record = record;
+    a.collide = 1;
+    CK(launch_forward(h.Q, coll_kind(h), h.storage, a, grid_for(h), h.stream));
+    h.parity ^= 1;
+    h.pending = h.n_ports > 0;
+    ++h.t;
+}
+
+// Load-only pass of the current state (admission reductions and/or record).
+void inspect(lbm_handle& h, StepDiag* diag, float* record) {
+    FwdArgs a = fwd_args(h);
+    a.parity = h.parity;
+    a.apply_ports = h.pending ? 1 : 0;
+    a.diag = diag;
+    a.record = record;
+    a.collide = 0;
+    CK(launch_forward(h.Q, coll_kind(h), h.storage, a, grid_for(h), h.stream));
+}
+
+void init_state(lbm_handle& h) {
+    CK(launch_init(h.Q, h.storage, h.G, h.P, h.pop.p, h.mask.as<uint32_t>(), h.stream));
+    h.parity = 0;
+    h.pending = false;
+    h.t = 0;
+    h.state_valid = true;
+}
+
+void require_design(const lbm_handle& h) {
+    if (!h.design_set) throw StateError("lbm_set_design must be called before stepping");
+}
+
+// Admission from the per-state records (solver.rs:708-793).
+lbm_status admit(lbm_handle& h, const std::vector<StepDiag>& d, lbm_diag_t* out, double ms) {
+    const size_t T = d.size();
+    bool nonfinite = false;
+    double minimum = INFINITY, maxu2 = 0;
+    for (auto& s : d) {
+        nonfinite = nonfinite || s.nonfinite;
+        minimum = std::min(minimum, (double)s.min_f);
+        maxu2 = std::max(maxu2, (double)s.max_u2);
+    }
+    const double mach = std::sqrt(maxu2) * std::sqrt(3.0);
+    const bool use_changes = h.n_ports > 0;
+    double cum = 0, err = 0, total = 0;
+    bool changes_finite = true;
+    const double m0 = (double)h.fluid_cells + d[0].mass_hi + d[0].mass_lo;
+    for (size_t t = 0; t < T; ++t) {
+        double mt = (double)h.fluid_cells + d[t].mass_hi + d[t].mass_lo;
+        if (t > 0 && use_changes) {
+            double e = d[t].exch_hi + d[t].exch_lo;
+            changes_finite = changes_finite && std::isfinite(e);
+            cum += e;
+            total += e;
+        }
+        err = std::max(err, std::fabs(mt - (m0 + cum)));
+    }
+    err /= m0;
+    if (out) {
+        out->maximum_mach = mach;
+        out->relative_mass_drift = err;
+        out->relaxation_time = h.tau;
+        out->minimum_population = minimum;
+        out->boundary_exchange_total = use_changes ? total : 0.0;
+        out->steps = (int64_t)T - 1;
+        out->nonfinite = nonfinite ? 1 : 0;
+        out->admitted = 0;
+        out->device_ms = ms;
+    }
+    if (nonfinite || !(minimum > 0)) throw ContractError("LBM trajectory has nonpositive or nonfinite populations");
+    if (!changes_finite) throw ContractError("Invalid boundary mass exchange history");
+    if (mach > h.mach_limit || err > 1e-6)
+        throw ContractError("LBM trajectory rejected: Mach=" + repr_float(mach) + ", mass drift=" + repr_float(err));
+    if (out) out->admitted = 1;
+    return LBM_OK;
+}
+
+// Runs `steps` steps from the current state with admission of every state
+// including the current one.  Optionally stores checkpoints every K steps.
+lbm_status run_admitted(lbm_handle& h, int64_t steps, lbm_diag_t* out, int64_t K) {
+    require_design(h);
+    int64_t* ctr = &h.device_bytes;
+    h.diag.alloc((size_t)(steps + 1) * sizeof(StepDiag), ctr);
+    StepDiag* d = h.diag.as<StepDiag>();
+    CK(cudaEventRecord(h.ev0, h.stream));
+    for (int64_t s = 0; s < steps; ++s) {
+        if (K > 0 && s % K == 0) {
+            // checkpoint of the state entering step s (scan.rs:181-196)
+            Checkpoint c;
+            c.buf = std::make_unique<DevBuf>();
+            c.buf->alloc(h.pop.bytes, ctr);
+            CK(cudaMemcpyAsync(c.buf->p, h.pop.p, h.pop.bytes, cudaMemcpyDeviceToDevice, h.stream));
+            c.t = h.t;
+            c.parity = h.parity;
+            c.pending = h.pending;
+            h.ckpts.push_back(std::move(c));
+        }
+        step(h, d + s, nullptr);
+    }
+    inspect(h, d + steps, nullptr);
+    CK(cudaEventRecord(h.ev1, h.stream));
+    std::vector<StepDiag> hd((size_t)steps + 1);
+    CK(cudaMemcpyAsync(hd.data(), d, hd.size() * sizeof(StepDiag), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, h.ev0, h.ev1));
+    return admit(h, hd, out, ms);
+}
+
+void ensure_scratch(lbm_handle& h) { h.scratch.alloc((size_t)h.n() * h.Q * sizeof(float), &h.device_bytes); }
+
+ObjArgs obj_args(lbm_handle& h) {
+    ObjArgs a{};
+    a.G = h.G;
+    a.P = h.P;
+    a.pop = h.pop.p;
+    a.mask = h.mask.as<uint32_t>();
+    a.alpha = h.alpha.as<float>();
+    a.phi = h.phi.as<float>();
+    a.ports = h.ports_d.as<PortMap>();
+    a.parity = h.parity;
+    a.apply_ports = h.pending ? 1 : 0;
+    a.tau = (float)h.tau;
+    a.vel = (float)(h.dx / h.dt);
+    a.dens = (float)h.density;
+    a.dt_s = (float)h.dt;
+    a.red = reduce_of(h);
+    return a;
+}
+
+double visc_scale(const lbm_handle& h) { return h.density * std::pow(h.dx, 5) / std::pow(h.dt, 3); }
+
+void responses(lbm_handle& h, double* out8, float* fields) {
+    ObjArgs a = obj_args(h);
+    a.sums = h.sums.as<double>();
+    a.fields = fields;
+    CK(launch_objective(h.Q, h.storage, LBM_STORE_F32, 0, a, grid_for(h), h.stream));
+    double s[16];
+    CK(cudaMemcpyAsync(s, h.sums.p, sizeof(s), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    double v[8];
+    for (int k = 0; k < 8; ++k) v[k] = s[2 * k] + s[2 * k + 1];
+    const double nf = (double)h.fluid_cells, dv = h.dx * h.dx * h.dx;
+    out8[0] = v[0] / nf;
+    out8[1] = v[1] / nf;
+    out8[2] = v[2] / nf;
+    out8[3] = 0.5 * v[3] * dv;
+    out8[4] = v[4] * dv;
+    out8[5] = v[5] * dv;
+    out8[6] = (h.n_inlet > 0 && h.n_outlet > 0) ? v[6] : 0.0;
+    out8[7] = v[7] * visc_scale(h);
+}
+
+DesignArgs design_args(lbm_handle& h) {
+    DesignArgs a{};
+    a.G = h.G;
+    a.raw = h.raw.as<float>();
+    a.cls = h.cls_d.as<uint8_t>();
+    a.fixed = h.fixed_d.as<float>();
+    a.offsets = h.offsets_d.as<int4>();
+    a.n_offsets = (int)h.offsets.size();
+    a.beta = h.beta;
+    a.eta = h.eta;
+    a.proj_a = h.proj_a;
+    a.proj_den = h.proj_den;
+    a.ramp_c = (float)(h.dt * h.drag_max * h.drag_shape);
+    a.ramp_q = (float)h.drag_shape;
+    a.phi = h.phi.as<float>();
+    a.alpha = h.alpha.as<float>();
+    a.den = h.den.as<float>();
+    a.slope = h.slope.as<float>();
+    return a;
+}
+
+// phi_bar -> raw gradient on the device (grad buffer), scaled abar optional.
+void design_transpose(lbm_handle& h, const float* phibar, const float* abar, float abar_scale,
+                      const float* abar_final) {
+    int64_t* ctr = &h.device_bytes;
+    h.scale.alloc((size_t)h.n() * 4, ctr);
+    h.grad.alloc((size_t)h.n() * 4, ctr);
+    DesignArgs a = design_args(h);
+    a.phibar = phibar;
+    a.abar = abar;
+    a.abar_scale = abar_scale;
+    a.abar_final = abar_final;
+    a.scale = h.scale.as<float>();
+    a.grad = h.grad.as<float>();
+    const int grid = (int)std::min<int64_t>((h.n() + 255) / 256, (int64_t)h.sms * 8);
+    CK(launch_sens_scale(a, grid, h.stream));
+    CK(launch_filter_transpose(a, grid, h.stream));
+}
+
+// ------------------------------------------------------------ adjoint
+struct AdjState {
+    int parity = 1;         // the first adjoint step after a seed gathers (parity 1)
+    float scale = 1.f;      // stored = true * scale for the lambda now in memory
+    float target = 1.f;     // scale the next adjoint step writes with
+    float s0 = 1.f;         // abar is accumulated in units of 1/s0
+    bool first = true;
+    int64_t steps = 0;
+};
+
+AdjArgs adj_args(lbm_handle& h) {
+    AdjArgs a{};
+    a.G = h.G;
+    a.P = h.P;
+    a.lam = h.lam.p;
+    a.mask = h.mask.as<uint32_t>();
+    a.alpha = h.alpha.as<float>();
+    a.ports = h.ports_d.as<PortMap>();
+    a.abar = h.abar.as<float>();
+    a.red = reduce_of(h);
+    return a;
+}
+
+// One transposed step linearised at record slot `rec`; returns nothing, the
+// norm (if requested) lands in norm2[0..1].
+void adjoint_step(lbm_handle& h, AdjState& st, const float* rec, bool want_norm) {
+    AdjArgs a = adj_args(h);
+    a.record = rec;
+    a.parity = st.parity;
+    a.port_transpose = 1;
+    a.overwrite_abar = st.first ? 1 : 0;
+    a.in_scale_inv = 1.f / st.scale;
+    a.out_scale = st.target;
+    a.abar_factor = st.s0;
+    a.norm2 = want_norm ? h.norm2.as<double>() : nullptr;
+    CK(launch_adjoint(h.Q, coll_kind(h), h.lam_storage, a, grid_for(h), h.stream));
+    st.parity ^= 1;
+    st.scale = st.target;
+    st.first = false;
+    ++st.steps;
+}
+
+double read_norm(lbm_handle& h) {
+    double s[2];
+    CK(cudaMemcpyAsync(s, h.norm2.p, sizeof(s), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    return std::sqrt(std::max(0.0, s[0] + s[1]));
+}
+
+// Objective VJP at the current state: lambda seed, abar_final, phibar and
+// the (rho, u) record.  Returns |mu_0| (true units).
+double seed(lbm_handle& h, const double* w, AdjState& st, float* record) {
+    int64_t* ctr = &h.device_bytes;
+    const int64_t n = h.n();
+    h.abar_final.alloc((size_t)n * 4, ctr);
+    h.phibar.alloc((size_t)n * 4, ctr);
+    h.norm2.alloc(2 * sizeof(double), ctr);
+    ObjArgs a = obj_args(h);
+    const double nf = (double)h.fluid_cells, dv = h.dx * h.dx * h.dx;
+    a.w[0] = w[0] / nf;
+    a.w[1] = w[1] / nf;
+    a.w[2] = w[2] / nf;
+    a.w[3] = 0.5 * w[3] * dv;
+    a.w[4] = w[4] * dv;
+    a.w[5] = w[5] * dv;
+    a.w[6] = (h.n_inlet > 0 && h.n_outlet > 0) ? w[6] : 0.0;
+    a.w[7] = w[7] * visc_scale(h);
+    a.lam = h.lam.p;
+    a.abar_final = h.abar_final.as<float>();
+    a.phibar = h.phibar.as<float>();
+    a.record = record;
+    a.port_transpose = 1;
+    a.norm2 = h.norm2.as<double>();
+    a.write_lambda = 0;
+    a.lam_scale = 1.f;
+    CK(launch_objective(h.Q, h.storage, h.lam_storage, 1, a, grid_for(h), h.stream));
+    const double n0 = read_norm(h);
+    const double entries = (double)h.fluid_cells * h.Q;
+    st.s0 = n0 > 0 ? (float)(std::sqrt(entries) / n0) : 1.f;
+    if (!std::isfinite(st.s0) || st.s0 == 0.f) st.s0 = 1.f;
+    st.scale = st.s0;
+    st.target = st.s0;
+    a.write_lambda = 1;
+    a.lam_scale = st.s0;
+    a.norm2 = nullptr;
+    a.record = nullptr;
+    CK(launch_objective(h.Q, h.storage, h.lam_storage, 1, a, grid_for(h), h.stream));
+    st.parity = 1;
+    st.first = true;
+    return n0;
+}
+
+void alloc_adjoint(lbm_handle& h, int lam_storage) {
+    int64_t* ctr = &h.device_bytes;
+    const int64_t n = h.n();
+    if (h.lam.p && h.lam_storage != lam_storage) h.lam.reset();
+    h.lam_storage = lam_storage;
+    h.lam.alloc((size_t)n * h.Q * storage_bytes(lam_storage), ctr);
+    h.abar.alloc((size_t)n * 4, ctr);
+    h.norm2.alloc(2 * sizeof(double), ctr);
+}
+
+float next_scale(const lbm_handle& h, double true_norm, float cur) {
+    if (!(true_norm > 0) || !std::isfinite(true_norm)) return cur;
+    double s = std::sqrt((double)h.fluid_cells * h.Q) / true_norm;
+    if (!std::isfinite(s) || s <= 0 || s > 3e38) return cur;
+    return (float)s;
+}
+
+void finish_gradient(lbm_handle& h, const AdjState& st, bool any_adjoint, double* grad) {
+    design_transpose(h, h.phibar.as<float>(), any_adjoint ? h.abar.as<float>() : nullptr, 1.f / st.s0,
+                     h.abar_final.as<float>());
+    std::vector<float> g((size_t)h.n());
+    CK(cudaMemcpyAsync(g.data(), h.grad.p, g.size() * 4, cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    bool finite = true;
+    for (int64_t x = 0; x < h.n(); ++x) {
+        grad[x] = g[x];
+        finite = finite && std::isfinite(g[x]);
+    }
+    if (!finite) throw ContractError("Nonfinite LBM sensitivity");
+}
+
+lbm_status gradient_steady(lbm_handle& h, const double* w, const lbm_adjoint_opts_t& o, double* grad,
+                           lbm_adjoint_report_t* rep) {
+    if (!h.forward_done) throw StateError("lbm_forward must succeed before lbm_gradient");
+    alloc_adjoint(h, o.lambda_storage);
+    int64_t* ctr = &h.device_bytes;
+    h.record.alloc((size_t)h.n() * 4 * sizeof(float), ctr);
+    AdjState st;
+    CK(cudaEventRecord(h.ev0, h.stream));
+    const double n0 = seed(h, w, st, h.record.as<float>());
+    double resid = 0;
+    bool converged = (n0 == 0);
+    const int64_t check = o.check_every > 0 ? o.check_every : 50;
+    const int64_t cap = o.max_iterations > 0 ? o.max_iterations : 100000;
+    float ms_adj = 0;
+    if (!converged) {
+        cudaEvent_t e2, e3;
+        CK(cudaEventCreate(&e2));
+        CK(cudaEventCreate(&e3));
+        CK(cudaEventRecord(e2, h.stream));
+        while (st.steps < cap) {
+            const int64_t chunk = std::min(check, cap - st.steps);
+            for (int64_t i = 0; i < chunk; ++i) adjoint_step(h, st, h.record.as<float>(), i == chunk - 1);
+            const double nrm = read_norm(h) / st.scale;
+            resid = nrm / n0;
+            if (resid <= o.tolerance) {
+                converged = true;
+                break;
+            }
+            // keep the stored adjoint near unit RMS (the 16-bit formats need
+            // it; the next step reads with the old scale, writes with the new)
+            st.target = next_scale(h, nrm, st.scale);
+        }
+        CK(cudaEventRecord(e3, h.stream));
+        CK(cudaEventSynchronize(e3));
+        CK(cudaEventElapsedTime(&ms_adj, e2, e3));
+        cudaEventDestroy(e2);
+        cudaEventDestroy(e3);
+    }
+    cudaEvent_t e4;
+    CK(cudaEventCreate(&e4));
+    CK(cudaEventRecord(e4, h.stream));
+    finish_gradient(h, st, st.steps > 0, grad);
+    float ms_sens = 0;
+    CK(cudaEventRecord(h.ev1, h.stream));
+    CK(cudaEventSynchronize(h.ev1));
+    CK(cudaEventElapsedTime(&ms_sens, e4, h.ev1));
+    cudaEventDestroy(e4);
+    if (rep) {
+        rep->residual = resid;
+        rep->iterations = st.steps;
+        rep->forward_recomputed = 0;
+        rep->peak_state_bytes = (int64_t)(h.record.bytes + h.lam.bytes);
+        rep->converged = converged ? 1 : 0;
+        rep->forward_ms = 0;
+        rep->adjoint_ms = ms_adj;
+        rep->sensitivity_ms = ms_sens;
+    }
+    if (!converged)
+        throw ConvergenceError("steady adjoint did not reach the residual tolerance within max_iterations (residual=" +
+                               repr_float(resid) + ")");
+    return LBM_OK;
+}
+
+lbm_status gradient_horizon(lbm_handle& h, const double* w, const lbm_adjoint_opts_t& o, double* grad,
+                            lbm_adjoint_report_t* rep) {
+    require_design(h);
+    const int64_t T = h.step_count;
+    int64_t K = o.checkpoint_every;
+    if (K <= 0) {
+        K = 1;
+        while (K * K < T) ++K;
+    }
+    K = std::min(K, T);
+    alloc_adjoint(h, o.lambda_storage);
+    int64_t* ctr = &h.device_bytes;
+    const size_t rec_bytes = (size_t)h.n() * 4 * sizeof(float);
+    if (o.record_budget_bytes > 0 && (int64_t)(rec_bytes * K) > o.record_budget_bytes)
+        throw ContractError("checkpoint interval needs more record memory than record_budget_bytes");
+    h.record.alloc(rec_bytes * (size_t)K, ctr);
+    h.ckpts.clear();
+    // forward with checkpoints, then admission (the reference re-runs parts())
+    init_state(h);
+    cudaEvent_t ef0, ef1;
+    CK(cudaEventCreate(&ef0));
+    CK(cudaEventCreate(&ef1));
+    lbm_diag_t dg{};
+    run_admitted(h, T, &dg, K);
+    h.forward_done = true;
+    AdjState st;
+    const double n0 = seed(h, w, st, nullptr);
+    float* rec = h.record.as<float>();
+    const size_t rec_stride = (size_t)h.n() * 4;
+    int64_t recomputed = 0;
+    float ms_fwd = 0, ms_adj = 0;
+    if (n0 > 0) {
+        cudaEvent_t ea0, ea1;
+        CK(cudaEventCreate(&ea0));
+        CK(cudaEventCreate(&ea1));
+        for (int64_t ci = (int64_t)h.ckpts.size() - 1; ci >= 0; --ci) {
+            Checkpoint& c = h.ckpts[ci];
+            const int64_t start = c.t, end = std::min(start + K, T);
+            CK(cudaMemcpyAsync(h.pop.p, c.buf->p, h.pop.bytes, cudaMemcpyDeviceToDevice, h.stream));
+            h.parity = c.parity;
+            h.pending = c.pending;
+            h.t = c.t;
+            CK(cudaEventRecord(ef0, h.stream));
+            for (int64_t t = start; t < end; ++t) {
+                float* r = rec + (size_t)(t - start) * rec_stride;
+                if (t + 1 < end) {
+                    step(h, nullptr, r);
+                    ++recomputed;
+                } else {
+                    inspect(h, nullptr, r);
+                }
+            }
+            CK(cudaEventRecord(ef1, h.stream));
+            CK(cudaEventRecord(ea0, h.stream));
+            for (int64_t t = end - 1; t >= start; --t) {
+                const bool last = (t == start);
+                adjoint_step(h, st, rec + (size_t)(t - start) * rec_stride, last);
+            }
+            CK(cudaEventRecord(ea1, h.stream));
+            CK(cudaEventSynchronize(ea1));
+            float a1 = 0, a2 = 0;
+            CK(cudaEventElapsedTime(&a1, ef0, ef1));
+            CK(cudaEventElapsedTime(&a2, ea0, ea1));
+            ms_fwd += a1;
+            ms_adj += a2;
+            // rescale the stored adjoint at segment boundaries
+            st.target = next_scale(h, read_norm(h) / st.scale, st.scale);
+        }
+        cudaEventDestroy(ea0);
+        cudaEventDestroy(ea1);
+    }
+    cudaEventDestroy(ef0);
+    cudaEventDestroy(ef1);
+    int64_t peak = (int64_t)h.record.bytes;
+    for (auto& c : h.ckpts) peak += (int64_t)c.buf->bytes;
+    h.ckpts.clear();
+    // the current state is the one of checkpoint 0's segment end; re-mark
+    h.forward_done = false;
+    h.state_valid = false;
+    cudaEvent_t e4;
+    CK(cudaEventCreate(&e4));
+    CK(cudaEventRecord(e4, h.stream));
+    finish_gradient(h, st, st.steps > 0, grad);
+    float ms_sens = 0;
+    CK(cudaEventRecord(h.ev1, h.stream));
+    CK(cudaEventSynchronize(h.ev1));
+    CK(cudaEventElapsedTime(&ms_sens, e4, h.ev1));
+    cudaEventDestroy(e4);
+    if (rep) {
+        rep->residual = 0;
+        rep->iterations = st.steps;
+        rep->forward_recomputed = recomputed;
+        rep->peak_state_bytes = peak;
+        rep->converged = 1;
+        rep->forward_ms = ms_fwd;
+        rep->adjoint_ms = ms_adj;
+        rep->sensitivity_ms = ms_sens;
+    }
+    return LBM_OK;
+}
+
+template <typename F>
+lbm_status guarded(lbm_handle* h, F&& fn) {
+    if (!h) return LBM_E_STATE;
+    try {
+        h->err.clear();
+        return fn();
+    } catch (const ContractError& e) {
+        h->err = e.what();
+        return LBM_E_CONTRACT;
+    } catch (const ConvergenceError& e) {
+        h->err = e.what();
+        return LBM_E_CONVERGENCE;
+    } catch (const StateError& e) {
+        h->err = e.what();
+        return LBM_E_STATE;
+    } catch (const CudaError& e) {
+        h->err = e.what();
+        return LBM_E_CUDA;
+    } catch (const std::bad_alloc&) {
+        h->err = "host allocation failed";
+        return LBM_E_CUDA;
+    } catch (const std::exception& e) {
+        h->err = e.what();
+        return LBM_E_CUDA;
+    }
+}
+
+void check_n(const lbm_handle& h, size_t n, size_t expect, const char* what) {
+    if (n != expect) throw ContractError(std::string(what) + " must be a finite shape-matched array");
+}
+
+}  // namespace
+
+// ================================================================ C ABI
+extern "C" {
+
+int32_t lbm_abi_version(void) { return LBM_ABI_VERSION; }
+
+const char* lbm_last_error(const lbm_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+lbm_status lbm_create(const lbm_problem_t* problem, lbm_handle** out) {
+    if (!out) return LBM_E_CONTRACT;
+    *out = nullptr;
+    if (!problem) {
+        g_create_error = "problem must not be NULL";
+        return LBM_E_CONTRACT;
+    }
+    auto h = std::make_unique<lbm_handle>();
+    try {
+        validate_and_build(*h, *problem);
+    } catch (const ContractError& e) {
+        g_create_error = e.what();
+        return LBM_E_CONTRACT;
+    } catch (const CudaError& e) {
+        g_create_error = e.what();
+        return LBM_E_CUDA;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        return LBM_E_CUDA;
+    }
+    g_create_error.clear();
+    *out = h.release();
+    return LBM_OK;
+}
+
+void lbm_destroy(lbm_handle* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    h->ckpts.clear();
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+lbm_status lbm_info(const lbm_handle* h, lbm_info_t* out) {
+    if (!h || !out) return LBM_E_STATE;
+    out->cells = h->G.n;
+    out->fluid_cells = h->fluid_cells;
+    out->q = h->Q;
+    out->n_ports = h->n_ports;
+    out->tau = h->tau;
+    for (int d = 0; d < 3; ++d) out->acceleration_lattice[d] = h->a[d];
+    out->device_bytes = h->device_bytes;
+    return LBM_OK;
+}
+
+lbm_status lbm_set_design(lbm_handle* h, const double* raw, size_t n) {
+    return guarded(h, [&]() {
+        check_n(*h, n, (size_t)h->n(), "model:control");
+        std::vector<float> r(n);
+        for (size_t x = 0; x < n; ++x) {
+            double v = raw[x];
+            if (!std::isfinite(v) || v < 0.0 || v > 1.0)
+                throw ContractError("model:control must be a finite shape-matched array in [0,1]");
+            r[x] = (float)v;
+        }
+        CK(cudaMemcpyAsync(h->raw.p, r.data(), n * 4, cudaMemcpyHostToDevice, h->stream));
+        DesignArgs a = design_args(*h);
+        const int grid = (int)std::min<int64_t>((h->n() + 255) / 256, (int64_t)h->sms * 8);
+        CK(launch_design_map(a, grid, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        h->design_set = true;
+        h->forward_done = false;
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_get_design(lbm_handle* h, double* phi, double* alpha) {
+    return guarded(h, [&]() {
+        require_design(*h);
+        std::vector<float> b((size_t)h->n());
+        if (phi) {
+            CK(cudaMemcpy(b.data(), h->phi.p, b.size() * 4, cudaMemcpyDeviceToHost));
+            for (size_t x = 0; x < b.size(); ++x) phi[x] = b[x];
+        }
+        if (alpha) {
+            CK(cudaMemcpy(b.data(), h->alpha.p, b.size() * 4, cudaMemcpyDeviceToHost));
+            for (size_t x = 0; x < b.size(); ++x) alpha[x] = b[x];
+        }
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_forward(lbm_handle* h, int64_t steps, lbm_diag_t* diag) {
+    return guarded(h, [&]() {
+        require_design(*h);
+        h->forward_done = false;
+        h->ckpts.clear();
+        init_state(*h);
+        const int64_t T = steps > 0 ? steps : h->step_count;
+        lbm_status s = run_admitted(*h, T, diag, 0);
+        h->forward_done = true;
+        return s;
+    });
+}
+
+lbm_status lbm_advance(lbm_handle* h, int64_t steps, lbm_diag_t* diag) {
+    return guarded(h, [&]() {
+        if (!h->state_valid) throw StateError("no current state: call lbm_forward or lbm_set_populations first");
+        if (steps < 0) throw ContractError("steps must be non-negative");
+        lbm_status s = run_admitted(*h, steps, diag, 0);
+        h->forward_done = true;
+        return s;
+    });
+}
+
+lbm_status lbm_set_populations(lbm_handle* h, const double* f, size_t n) {
+    return guarded(h, [&]() {
+        const int64_t N = h->n();
+        const int Q = h->Q;
+        check_n(*h, n, (size_t)(N * Q), "populations");
+        std::vector<float> g((size_t)N * Q);
+        for (int64_t x = 0; x < N; ++x)
+            for (int q = 0; q < Q; ++q) g[(size_t)q * N + x] = (float)(f[x * Q + q] - h->L.w[q]);
+        ensure_scratch(*h);
+        CK(cudaMemcpyAsync(h->scratch.p, g.data(), g.size() * 4, cudaMemcpyHostToDevice, h->stream));
+        const int grid = grid_for(*h);
+        CK(launch_upload_pop(Q, h->storage, h->G, h->pop.p, h->scratch.as<float>(), grid, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        h->parity = 0;
+        h->pending = false;
+        h->t = 0;
+        h->state_valid = true;
+        h->forward_done = false;
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_get_populations(lbm_handle* h, double* f, size_t n) {
+    return guarded(h, [&]() {
+        if (!h->state_valid) throw StateError("no current state");
+        const int64_t N = h->n();
+        const int Q = h->Q;
+        check_n(*h, n, (size_t)(N * Q), "populations");
+        ensure_scratch(*h);
+        CK(launch_canon_pop(Q, h->storage, h->G, h->pop.p, h->mask.as<uint32_t>(), h->ports_d.as<PortMap>(),
+                            h->parity, h->pending ? 1 : 0, h->scratch.as<float>(), grid_for(*h), h->stream));
+        std::vector<float> g((size_t)N * Q);
+        CK(cudaMemcpyAsync(g.data(), h->scratch.p, g.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (int64_t x = 0; x < N; ++x)
+            for (int q = 0; q < Q; ++q) f[x * Q + q] = h->L.w[q] + (double)g[(size_t)q * N + x];
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_responses(lbm_handle* h, double* out8) {
+    return guarded(h, [&]() {
+        if (!h->state_valid) throw StateError("no current state");
+        require_design(*h);
+        responses(*h, out8, nullptr);
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_fields(lbm_handle* h, double* density, double* velocity, double* pressure) {
+    return guarded(h, [&]() {
+        if (!h->state_valid) throw StateError("no current state");
+        require_design(*h);
+        const int64_t N = h->n();
+        ensure_scratch(*h);
+        double r8[8];
+        responses(*h, r8, h->scratch.as<float>());
+        std::vector<float> fl((size_t)N * 4);
+        CK(cudaMemcpyAsync(fl.data(), h->scratch.p, fl.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        const double vel = h->dx / h->dt;
+        const double unit = vel * vel / 3.0;
+        for (int64_t x = 0; x < N; ++x) {
+            const bool solid = h->cls[x] == 0;
+            // solid cells keep their equilibrium populations: rho = 1, u = 0
+            const double rp = solid ? 0.0 : (double)fl[x];
+            const double rho = (1.0 + rp) * h->density;
+            if (density) density[x] = rho;
+            if (pressure) pressure[x] = (rho - h->density) * unit;
+            if (velocity)
+                for (int d = 0; d < 3; ++d) velocity[3 * x + d] = solid ? 0.0 : (double)fl[(size_t)(d + 1) * N + x] * vel;
+        }
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_gradient(lbm_handle* h, const double* weights, const lbm_adjoint_opts_t* opts, double* grad,
+                        lbm_adjoint_report_t* report) {
+    return guarded(h, [&]() {
+        lbm_adjoint_opts_t o{};
+        o.mode = LBM_ADJ_HORIZON;
+        o.lambda_storage = LBM_STORE_F32;
+        o.checkpoint_every = 0;
+        o.max_iterations = 100000;
+        o.check_every = 50;
+        o.tolerance = 1e-8;
+        if (opts) o = *opts;
+        if (!weights || !grad) throw ContractError("weights and grad must not be NULL");
+        for (int k = 0; k < LBM_N_RESPONSES; ++k)
+            if (!std::isfinite(weights[k])) throw ContractError("response weights must be finite");
+        if (o.lambda_storage < LBM_STORE_F32 || o.lambda_storage > LBM_STORE_BF16)
+            throw ContractError("lambda_storage must be float32, float16 or bfloat16");
+        if (o.mode == LBM_ADJ_STEADY) {
+            if (!(o.tolerance > 0)) throw ContractError("steady adjoint tolerance must be positive");
+            return gradient_steady(*h, weights, o, grad, report);
+        }
+        if (o.mode != LBM_ADJ_HORIZON) throw ContractError("adjoint mode must be horizon or steady");
+        return gradient_horizon(*h, weights, o, grad, report);
+    });
+}
+
+lbm_status lbm_step_vjp(lbm_handle* h, const double* state, const double* lambda_next, double* lambda,
+                        double* alpha_bar, size_t n_populations) {
+    return guarded(h, [&]() {
+        require_design(*h);
+        const int64_t N = h->n();
+        const int Q = h->Q;
+        check_n(*h, n_populations, (size_t)(N * Q), "populations");
+        lbm_status s = lbm_set_populations(h, state, n_populations);
+        if (s != LBM_OK) throw ContractError(h->err);
+        int64_t* ctr = &h->device_bytes;
+        alloc_adjoint(*h, LBM_STORE_F32);
+        h->record.alloc((size_t)N * 4 * sizeof(float), ctr);
+        inspect(*h, nullptr, h->record.as<float>());
+        std::vector<float> v((size_t)N * Q);
+        for (int64_t x = 0; x < N; ++x)
+            for (int q = 0; q < Q; ++q) v[(size_t)q * N + x] = (float)lambda_next[x * Q + q];
+        ensure_scratch(*h);
+        CK(cudaMemcpyAsync(h->scratch.p, v.data(), v.size() * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(launch_seed_lam(Q, LBM_STORE_F32, h->G, h->lam.p, h->mask.as<uint32_t>(), h->ports_d.as<PortMap>(),
+                           h->scratch.as<float>(), 1.f, 1, grid_for(*h), h->stream));
+        AdjArgs a = adj_args(*h);
+        a.record = h->record.as<float>();
+        a.parity = 1;
+        a.port_transpose = 0;
+        a.overwrite_abar = 1;
+        a.in_scale_inv = 1.f;
+        a.out_scale = 1.f;
+        a.abar_factor = 1.f;
+        CK(launch_adjoint(Q, coll_kind(*h), LBM_STORE_F32, a, grid_for(*h), h->stream));
+        CK(launch_canon_lam(Q, LBM_STORE_F32, h->G, h->lam.p, h->mask.as<uint32_t>(), 1, 1.f, h->scratch.as<float>(),
+                            grid_for(*h), h->stream));
+        CK(cudaMemcpyAsync(v.data(), h->scratch.p, v.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+        std::vector<float> ab((size_t)N);
+        CK(cudaMemcpyAsync(ab.data(), h->abar.p, ab.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (int64_t x = 0; x < N; ++x) {
+            for (int q = 0; q < Q; ++q) lambda[x * Q + q] = v[(size_t)q * N + x];
+            if (alpha_bar) alpha_bar[x] = h->cls[x] == 0 ? 0.0 : (double)ab[x];
+        }
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_design_vjp(lbm_handle* h, const double* phi_bar, double* out, size_t n) {
+    return guarded(h, [&]() {
+        require_design(*h);
+        check_n(*h, n, (size_t)h->n(), "phi_bar");
+        int64_t* ctr = &h->device_bytes;
+        h->phibar.alloc(n * 4, ctr);
+        std::vector<float> v(n);
+        for (size_t x = 0; x < n; ++x) v[x] = (float)phi_bar[x];
+        CK(cudaMemcpyAsync(h->phibar.p, v.data(), n * 4, cudaMemcpyHostToDevice, h->stream));
+        design_transpose(*h, h->phibar.as<float>(), nullptr, 1.f, nullptr);
+        CK(cudaMemcpyAsync(v.data(), h->grad.p, n * 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (size_t x = 0; x < n; ++x) out[x] = v[x];
+        return LBM_OK;
+    });
+}
+
+}  // extern "C"

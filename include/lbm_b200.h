@@ -1,0 +1,293 @@
+/*
+ * lbm_b200.h -- C-ABI of the B200 (sm_100a) differentiable lattice-Boltzmann
+ * density-design solver.
+ *
+ * This library is the GPU implementation of the reference provider
+ * `lattice_boltzmann_d3q19` of implexity-physics-lbm, extended with the TRT and
+ * MRT collision operators and the D3Q27 lattice of the reference's moving
+ * engine.  A host (the reference's Rust provider through a `-sys` crate, the
+ * Python binding in implexity_b200/, or any C/C++ caller) hands it a normalised
+ * problem description, a raw design field, and asks for the forward trajectory,
+ * the responses and the discrete-adjoint design gradient.
+ *
+ * Reference interface each entry point replaces (paths inside the reference
+ * project):
+ *   lbm_create        LbmProblem::normalize        crates/implexity-physics-lbm/src/solver.rs:414-550
+ *                     normalize_ports / CompiledPort::new  src/ports.rs:106-272, 509-521
+ *                     DesignMap::new               src/design.rs:109-171
+ *                     Streaming::new               src/solver.rs:84-119
+ *   lbm_set_design    LbmProblem::checked_design / fraction / resistance  src/solver.rs:562-590
+ *   lbm_forward       LbmProblem::history + admit  src/solver.rs:677-687, 708-793
+ *   lbm_responses     LbmProblem::vector           src/solver.rs:874-893
+ *   lbm_fields        LbmProblem::fields / flow_fields  src/solver.rs:689-705, src/provider.rs:267-282
+ *   lbm_gradient      sensitivities_value chain    src/provider.rs:332-365
+ *                     (vector_vjp solver.rs:896-947, history_adjoint :798-815,
+ *                      DesignMap::vjp design.rs:219-243)
+ *   lbm_set_populations / lbm_get_populations / lbm_advance
+ *                     TimeStepper::{initial_state, advance}  implexity-solve/src/time_stepper.rs:81-148
+ *   lbm_step_vjp      LbmProblem::interval_vjp     src/solver.rs:642-674
+ *
+ * Conventions
+ *   - Cells are indexed like the reference Grid: cell = (i*ny + j)*nz + k
+ *     (d3q19.rs:87-89), i.e. C order of an array of shape (nx, ny, nz).
+ *   - Host population arrays are FP64, cell-major: f[cell*Q + q], with the
+ *     velocity ordering of d3q19.rs:29-51 (D3Q19) or moving/lattice.rs:93-121
+ *     (D3Q27).
+ *   - Host arrays passed in are borrowed for the duration of the call only.
+ *   - Every call is synchronous at return and runs on the handle's own CUDA
+ *     stream.  A handle must be used by one host thread at a time.
+ *   - No exception or abort crosses this ABI.  A failing call returns a
+ *     status and leaves a message readable with lbm_last_error().
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define LBM_API __attribute__((visibility("default")))
+#else
+#define LBM_API
+#endif
+
+/* Status codes.  LBM_E_CONTRACT mirrors CaeError::Contract and carries the
+ * reference's own messages (implexity-core/src/error.rs:34-56); the reference
+ * reports trajectory admission failures as contract errors too
+ * (solver.rs:717-771).  LBM_E_CONVERGENCE is used by the steady adjoint when
+ * it reaches its iteration cap. */
+typedef enum {
+    LBM_OK = 0,
+    LBM_E_CONTRACT = 1,
+    LBM_E_CONVERGENCE = 2,
+    LBM_E_CUDA = 3,
+    LBM_E_STATE = 4 /* call order: e.g. responses requested before a forward run */
+} lbm_status;
+
+typedef enum { LBM_D3Q19 = 19, LBM_D3Q27 = 27 } lbm_lattice;
+
+/* Collision operators (moving/collision.rs:38-53).  BGK is the reference
+ * density-design provider's operator (solver.rs:298-322); TRT and MRT are the
+ * moving engine's, with Guo forcing and the implicit half-step Brinkman
+ * velocity of moving/psm.rs:213-226. */
+typedef enum { LBM_BGK = 0, LBM_TRT = 1, LBM_MRT = 2 } lbm_collision;
+
+/* Storage type of the populations on the device.  Arithmetic is FP32 in all
+ * cases; the 16-bit variants store (f_q - w_q)/w_q. */
+typedef enum { LBM_STORE_F32 = 0, LBM_STORE_F16 = 1, LBM_STORE_BF16 = 2 } lbm_storage;
+
+typedef enum { LBM_PORT_VELOCITY = 0, LBM_PORT_PRESSURE = 1 } lbm_port_kind;
+
+/* Faces in the order of ports.rs FACES: xmin, xmax, ymin, ymax, zmin, zmax. */
+typedef enum {
+    LBM_XMIN = 0, LBM_XMAX = 1, LBM_YMIN = 2, LBM_YMAX = 3, LBM_ZMIN = 4, LBM_ZMAX = 5
+} lbm_face;
+
+/* Design filters.  CONIC is DesignMap's filter (design.rs:118-158): weights
+ * (r - |d|)_+ over editable in-box neighbours.  BOX is a uniform
+ * (2h+1)^3 average over the same neighbour set (h = half width in cells);
+ * it has no reference counterpart. */
+typedef enum { LBM_FILTER_CONIC = 0, LBM_FILTER_BOX = 1 } lbm_filter_kind;
+
+/* Responses (provider.rs:56-63) plus two with no reference counterpart:
+ * the inlet-outlet gauge pressure drop (mean over velocity-port cells minus
+ * mean over pressure-port cells) and the total viscous dissipation. */
+enum {
+    LBM_R_MEAN_UX = 0,
+    LBM_R_MEAN_UY = 1,
+    LBM_R_MEAN_UZ = 2,
+    LBM_R_KINETIC = 3,
+    LBM_R_POROUS_DISSIPATION = 4,
+    LBM_R_FLUID_VOLUME = 5,
+    LBM_R_PRESSURE_DROP = 6,
+    LBM_R_VISCOUS_DISSIPATION = 7,
+    LBM_N_RESPONSES = 8
+};
+
+#define LBM_MAX_PORTS 7
+
+/* One planar port (ports.rs:55-68, normalize_ports :106-272).  Only the
+ * default "legacy_moment" reconstruction (ports.rs:343-406) is provided. */
+typedef struct {
+    int32_t kind;             /* lbm_port_kind */
+    int32_t face;             /* lbm_face */
+    const uint8_t* mask;      /* N booleans, the full-grid port mask */
+    double velocity_m_s[3];
+    double gauge_pressure_Pa; /* pressure ports only */
+} lbm_port_t;
+
+/* The problem mapping of solver.rs:46-65 after JSON parsing (key sets and
+ * array shapes are the host's job), plus the collision/lattice/storage options
+ * of the moving engine (moving/field.rs:79-191).  lbm_create applies the
+ * reference's numeric validation with its messages. */
+typedef struct {
+    int32_t lattice;          /* lbm_lattice */
+    int32_t collision;        /* lbm_collision */
+    int32_t storage;          /* lbm_storage */
+    int32_t shape[3];
+    int32_t periodic_axes[3]; /* booleans; false = closed halfway bounce-back walls */
+    int32_t n_ports;
+    int64_t step_count;
+    double spacing_m;
+    double step_s;
+    double density_kg_m3;
+    double kinematic_viscosity_m2_s;
+    double acceleration_m_s2[3];
+    double drag_max_per_s;
+    double drag_shape;
+    double mach_limit;
+    /* topology map (design.rs:37-93) */
+    double filter_radius_m;
+    double projection_beta;
+    double projection_eta;
+    int32_t filter_kind;      /* lbm_filter_kind */
+    int32_t box_half_width;   /* cells, LBM_FILTER_BOX only */
+    /* collision parameters (moving/collision.rs:36-53); NaN = "None" */
+    double trt_magic;         /* TRT magic parameter, default 3/16 */
+    double mrt_odd_magic;     /* MRT odd-moment magic, default 3/16 */
+    double mrt_bulk_rate;     /* NaN -> shear rate */
+    double mrt_even_rate;     /* NaN -> shear rate */
+    const uint8_t* solid_mask;     /* N */
+    const uint8_t* design_region;  /* N */
+    const double* fixed_design;    /* N, in [0,1] */
+    const lbm_port_t* ports;       /* n_ports entries */
+} lbm_problem_t;
+
+/* Trajectory admission record (solver.rs:708-793).  Filled by lbm_forward
+ * and lbm_advance. */
+typedef struct {
+    double maximum_mach;          /* sqrt(3) * max |u| over fluid cells and states */
+    double relative_mass_drift;   /* max_t |M_t - (M_0 + sum exchange)| / M_0 */
+    double relaxation_time;       /* tau */
+    double minimum_population;    /* over fluid cells and states */
+    double boundary_exchange_total; /* lattice mass exchanged by ports */
+    int64_t steps;
+    int32_t nonfinite;            /* any non-finite population seen */
+    int32_t admitted;             /* 1 if the reference admission passes */
+    double device_ms;             /* CUDA-event time of the stepping kernels */
+} lbm_diag_t;
+
+/* Adjoint modes.  HORIZON is the reference's fixed-horizon discrete adjoint
+ * of all step_count steps (history_adjoint, solver.rs:798-815), with the
+ * forward recomputed from checkpoints every `checkpoint_every` steps
+ * (implexity-ad/src/scan.rs:140-246, Checkpointing::Every).  STEADY linearises
+ * one step at the final state and sums the Neumann series of the transposed
+ * step until the relative norm of the newest term is below `tolerance`
+ * (implexity-ad/src/implicit.rs:49-67 semantics). */
+typedef enum { LBM_ADJ_HORIZON = 0, LBM_ADJ_STEADY = 1 } lbm_adjoint_mode;
+
+typedef struct {
+    int32_t mode;             /* lbm_adjoint_mode */
+    int32_t lambda_storage;   /* lbm_storage of the adjoint populations */
+    int64_t checkpoint_every; /* HORIZON: K (<= 0 selects sqrt(step_count)) */
+    int64_t max_iterations;   /* STEADY: cap */
+    int64_t check_every;      /* STEADY: residual readback period */
+    double tolerance;         /* STEADY: relative residual */
+    int64_t record_budget_bytes; /* HORIZON: device bytes for per-step records (0 = auto) */
+} lbm_adjoint_opts_t;
+
+typedef struct {
+    double residual;              /* STEADY: final relative residual */
+    int64_t iterations;           /* adjoint steps taken */
+    int64_t forward_recomputed;   /* forward steps re-run from checkpoints */
+    int64_t peak_state_bytes;     /* checkpoint + record bytes held on device */
+    int32_t converged;
+    double forward_ms;            /* device time of the recomputation */
+    double adjoint_ms;            /* device time of the adjoint steps */
+    double sensitivity_ms;        /* device time of seed + design VJP */
+} lbm_adjoint_report_t;
+
+typedef struct lbm_handle lbm_handle;
+
+/* ---- lifetime ----------------------------------------------------------- */
+
+/* Validates and normalises the problem (LbmProblem::normalize), builds the
+ * link masks, port maps and design filter, and allocates the device buffers
+ * on the current CUDA device.  On failure *out is NULL and the message is
+ * available from lbm_last_error(NULL). */
+LBM_API lbm_status lbm_create(const lbm_problem_t* problem, lbm_handle** out);
+LBM_API void lbm_destroy(lbm_handle* h);
+
+/* Message of the last failing call on h (or of the last failing lbm_create
+ * in this thread when h is NULL).  Never NULL. */
+LBM_API const char* lbm_last_error(const lbm_handle* h);
+
+LBM_API int32_t lbm_abi_version(void);
+
+/* Normalised scalars: tau, lattice acceleration, cell count, Q. */
+typedef struct {
+    int64_t cells;
+    int64_t fluid_cells;
+    int32_t q;
+    int32_t n_ports;
+    double tau;
+    double acceleration_lattice[3];
+    int64_t device_bytes;     /* bytes allocated on the device by the handle */
+} lbm_info_t;
+LBM_API lbm_status lbm_info(const lbm_handle* h, lbm_info_t* out);
+
+/* ---- design ------------------------------------------------------------- */
+
+/* checked_design + fraction + resistance (solver.rs:562-590, design.rs:199-216,
+ * 284-286).  raw has N entries in [0,1]. */
+LBM_API lbm_status lbm_set_design(lbm_handle* h, const double* raw, size_t n);
+
+/* Copies the mapped fluid fraction phi and the Brinkman resistance alpha
+ * (per time step) to the host (either pointer may be NULL). */
+LBM_API lbm_status lbm_get_design(lbm_handle* h, double* phi, double* alpha);
+
+/* ---- forward -------------------------------------------------------------- */
+
+/* Initial populations (solver.rs:593-601) followed by `steps` steps
+ * (steps <= 0: the problem's step_count), with the admission reductions of
+ * every state.  Returns LBM_E_CONTRACT with the reference's messages when
+ * the trajectory is not admitted; diag is filled either way. */
+LBM_API lbm_status lbm_forward(lbm_handle* h, int64_t steps, lbm_diag_t* diag);
+
+/* TimeStepper-granular access.  lbm_set_populations loads a host state
+ * (f[cell*Q+q], FP64) as the current state; lbm_advance runs n more steps
+ * from the current state; lbm_get_populations returns the current state with
+ * the port reconstruction applied (the reference's "after" state). */
+LBM_API lbm_status lbm_set_populations(lbm_handle* h, const double* f, size_t n);
+LBM_API lbm_status lbm_get_populations(lbm_handle* h, double* f, size_t n);
+LBM_API lbm_status lbm_advance(lbm_handle* h, int64_t steps, lbm_diag_t* diag);
+
+/* The 8 responses of the current state (LBM_R_*), FP64 compensated sums. */
+LBM_API lbm_status lbm_responses(lbm_handle* h, double* out8);
+
+/* Physical fields of the current state (LbmProblem::fields, provider.rs
+ * flow_fields): density [N] kg/m^3, velocity [N*3] m/s, gauge pressure [N] Pa.
+ * Any pointer may be NULL. */
+LBM_API lbm_status lbm_fields(lbm_handle* h, double* density, double* velocity, double* pressure);
+
+/* ---- adjoint ------------------------------------------------------------ */
+
+/* Design gradient of sum_k weights[k] * response_k (weights has
+ * LBM_N_RESPONSES entries) with respect to the raw design, after a
+ * successful lbm_forward.  grad has N entries.  opts may be NULL (HORIZON,
+ * FP32 adjoint storage, K = sqrt(step_count)). */
+LBM_API lbm_status lbm_gradient(lbm_handle* h, const double* weights, const lbm_adjoint_opts_t* opts,
+                        double* grad, lbm_adjoint_report_t* report);
+
+/* One transposed step (interval_vjp without port-exchange cotangents):
+ * given a state f_t and the cotangent of f_{t+1}, returns the cotangent of
+ * f_t and the per-cell cotangent of alpha.  All arrays FP64 host,
+ * populations cell-major.  alpha_bar may be NULL. */
+LBM_API lbm_status lbm_step_vjp(lbm_handle* h, const double* state, const double* lambda_next,
+                        double* lambda, double* alpha_bar, size_t n_populations);
+
+/* Design-map transpose alone (DesignMap::vjp, design.rs:219-243) for the
+ * design last set: out[N] = d phi / d raw ^T phi_bar. */
+LBM_API lbm_status lbm_design_vjp(lbm_handle* h, const double* phi_bar, double* out, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBM_B200_H */

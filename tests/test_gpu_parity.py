@@ -1,0 +1,185 @@
+"""Parity of the CUDA library (through its C-ABI) with the FP64 oracle.
+
+Tolerances (FP32 arithmetic and storage unless stated):
+  populations / velocity / density   max |gpu - ref| / max |ref| <= 1e-5
+  responses                          relative 1e-5 (transverse mean velocities
+                                     against 1e-5 of the axial one)
+  one transposed step                relative L2 <= 1e-5
+  design gradient                    relative L2 <= 1e-4
+  FP16 storage                       velocity 2e-3, gradient relative L2 <= 1e-3
+"""
+import numpy as np
+import pytest
+
+from implexity_b200 import LbmSolver, normalize, workloads
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a, float).ravel(), np.asarray(b, float).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def rel_max(a, b):
+    a, b = np.asarray(a, float).ravel(), np.asarray(b, float).ravel()
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def macroscopic(f, q, alpha, a_lat):
+    """rho and the Brinkman-corrected velocity of populations f[cells, q]."""
+    from oracle.oracle import lib  # noqa: F401  (keeps the oracle build fresh)
+
+    if q == 19:
+        c = np.array(
+            [[0, 0, 0], [-1, -1, 0], [-1, 0, -1], [-1, 0, 0], [-1, 0, 1], [-1, 1, 0], [0, -1, -1], [0, -1, 0],
+             [0, -1, 1], [0, 0, -1], [0, 0, 1], [0, 1, -1], [0, 1, 0], [0, 1, 1], [1, -1, 0], [1, 0, -1], [1, 0, 0],
+             [1, 0, 1], [1, 1, 0]], float)
+    else:
+        c = np.array([[0, 0, 0]] + [[a, b, d] for a in (-1, 0, 1) for b in (-1, 0, 1) for d in (-1, 0, 1)
+                                    if (a, b, d) != (0, 0, 0)], float)
+    rho = f.sum(1)
+    u = (f @ c / rho[:, None] + 0.5 * np.asarray(a_lat)) / (1 + 0.5 * alpha[:, None])
+    return rho, u
+
+
+CASES = [
+    ("bgk", "D3Q19"),
+    ("trt", "D3Q19"),
+    ("mrt", "D3Q19"),
+    ("trt", "D3Q27"),
+    ("mrt", "D3Q27"),
+]
+
+
+def make(coll, lattice, shape=(16, 10, 8), steps=120, storage="float32", seed=1, **kw):
+    prob = workloads.channel_problem(
+        shape=shape, steps=steps, collision=coll, lattice=lattice, storage=storage,
+        mrt_bulk_rate=1.2 if coll == "mrt" else None, **kw,
+    )
+    norm = normalize(prob)
+    raw = workloads.uniform_design(norm.shape, seed)
+    return prob, norm, raw
+
+
+@pytest.mark.parametrize("coll,lattice", CASES)
+def test_forward_matches_oracle(gpu_lib, coll, lattice):
+    prob, norm, raw = make(coll, lattice)
+    o = Oracle(norm)
+    phi_ref, alpha_ref = o.design(raw)
+    f_ref, d_ref = o.history(alpha_ref, norm.step_count)
+    with LbmSolver(prob) as s:
+        s.set_design(raw)
+        phi, alpha = s.design()
+        assert rel_max(phi, phi_ref) < 1e-6
+        assert rel_max(alpha, alpha_ref) < 1e-5
+        d = s.forward()
+        f = s.populations()
+        assert rel_max(f, f_ref) < 1e-5
+        rho, u = macroscopic(f, s.q, alpha_ref, o.acceleration_lattice)
+        rho_r, u_r = macroscopic(f_ref, s.q, alpha_ref, o.acceleration_lattice)
+        assert rel_max(u, u_r) < 1e-5
+        assert np.max(np.abs(rho - rho_r)) < 1e-5
+        assert d.admitted and d_ref.admitted
+        assert abs(d.maximum_mach - d_ref.maximum_mach) < 1e-5 * d_ref.maximum_mach
+        assert abs(d.relative_mass_drift - d_ref.relative_mass_drift) < 1e-7
+        r = s.responses()
+        r_ref = o.vector(phi_ref, alpha_ref, f_ref)
+        for k in (0, 3, 4, 5, 6, 7):
+            assert abs(r[k] - r_ref[k]) <= 1e-5 * abs(r_ref[k]), (k, r[k], r_ref[k])
+        for k in (1, 2):
+            assert abs(r[k] - r_ref[k]) <= 1e-5 * abs(r_ref[0])
+
+
+@pytest.mark.parametrize("lattice", ["D3Q19", "D3Q27"])
+def test_periodic_solid_body_force(gpu_lib, lattice):
+    """Periodic x/z, closed y walls, solid obstacles next to periodic faces,
+    body force and no ports: the wrap and solid-neighbour bounce-back paths."""
+    shape = (12, 9, 8)
+    solid = np.zeros(shape, bool)
+    solid[0, 3:5, 0:2] = True
+    solid[6:8, 4, 3:6] = True
+    prob = workloads.channel_problem(shape=shape, steps=150, collision="trt", lattice=lattice, ports=False, solid=solid)
+    prob["periodic_axes"] = [True, False, True]
+    prob["acceleration_m_s2"] = [2e-5, 0.0, 1e-6]
+    prob["design_region"] = ~solid
+    prob["design_region"][:, 0, :] = False
+    norm = normalize(prob)
+    raw = workloads.uniform_design(shape, 4)
+    o = Oracle(norm)
+    phi_r, alpha_r = o.design(raw)
+    f_r, d_r = o.history(alpha_r, norm.step_count)
+    with LbmSolver(prob) as s:
+        s.set_design(raw)
+        d = s.forward()
+        f = s.populations()
+        assert rel_max(f, f_r) < 1e-5
+        assert d.admitted == bool(d_r.admitted)
+        assert abs(d.relative_mass_drift - d_r.relative_mass_drift) < 1e-7
+
+
+@pytest.mark.parametrize("coll,lattice", CASES)
+def test_step_vjp_matches_oracle(gpu_lib, coll, lattice):
+    prob, norm, raw = make(coll, lattice, steps=40)
+    o = Oracle(norm)
+    _, alpha = o.design(raw)
+    state, _ = o.history(alpha, 40)
+    rng = np.random.default_rng(7)
+    lam_next = rng.standard_normal(state.shape)
+    lam_ref, ab_ref = o.interval_vjp(state, alpha, lam_next)
+    with LbmSolver(prob) as s:
+        s.set_design(raw)
+        lam, ab = s.step_vjp(state, lam_next)
+    assert rel_l2(lam, lam_ref) < 1e-5
+    assert rel_l2(ab, ab_ref) < 1e-5
+
+
+@pytest.mark.parametrize("coll,lattice", [("bgk", "D3Q19"), ("trt", "D3Q19"), ("mrt", "D3Q27")])
+@pytest.mark.parametrize("response", [0, 3, 4, 5, 6, 7])
+def test_horizon_gradient_matches_oracle(gpu_lib, coll, lattice, response):
+    prob, norm, raw = make(coll, lattice, steps=60)
+    w = np.zeros(8)
+    w[response] = 1.0
+    o = Oracle(norm)
+    g_ref, r_ref, _, st = o.gradient(raw, w, mode="horizon", K=13)
+    assert st == 0
+    with LbmSolver(prob) as s:
+        s.set_design(raw)
+        g, rep = s.gradient(w, mode="horizon", checkpoint_every=13)
+    assert rep.iterations == 60
+    assert rel_l2(g, g_ref) < 1e-4, rel_l2(g, g_ref)
+
+
+def test_steady_gradient_matches_oracle(gpu_lib):
+    prob, norm, raw = make("trt", "D3Q19", steps=1500)
+    w = workloads.objective_weights()
+    o = Oracle(norm)
+    g_ref, r_ref, rep_ref, st = o.gradient(raw, w, mode="steady", tol=1e-12)
+    assert st == 0
+    with LbmSolver(prob) as s:
+        s.set_design(raw)
+        s.forward()
+        r = s.responses()
+        g, rep = s.gradient(w, mode="steady", tolerance=1e-8)
+    assert rep.converged
+    assert abs(np.dot(w, r) - np.dot(w, r_ref)) <= 1e-6 * abs(np.dot(w, r_ref)) + 1e-12
+    assert rel_l2(g, g_ref) < 1e-4, rel_l2(g, g_ref)
+
+
+def test_fp16_storage_close_to_fp32(gpu_lib):
+    prob32, norm, raw = make("trt", "D3Q19", steps=600)
+    prob16, _, _ = make("trt", "D3Q19", steps=600, storage="float16")
+    w = workloads.objective_weights()
+    with LbmSolver(prob32) as s32, LbmSolver(prob16) as s16:
+        for s in (s32, s16):
+            s.set_design(raw)
+            s.forward()
+        f32, f16 = s32.populations(), s16.populations()
+        _, alpha = s32.design()
+        _, u32 = macroscopic(f32, 19, alpha.ravel(), s32.acceleration_lattice)
+        _, u16 = macroscopic(f16, 19, alpha.ravel(), s16.acceleration_lattice)
+        assert rel_max(u16, u32) < 2e-3
+        g32, _ = s32.gradient(w, mode="steady", tolerance=1e-8)
+        g16, _ = s16.gradient(w, mode="steady", tolerance=1e-8, lambda_storage="float16")
+        assert rel_l2(g16, g32) < 1e-3, rel_l2(g16, g32)
