@@ -257,6 +257,31 @@ def run_gpu(args, rank, world, local):
     return results
 
 
+def run_profile_case(args):
+    """A short case of the bench kernels for ncu: forward steps and adjoint
+    iterations of the bench workload, no timing."""
+    import torch
+
+    from implexity_b200 import ConvergenceError, LbmSolver, normalize, workloads
+
+    torch.cuda.set_device(0)
+    shape, T, coll, bulk, dkind = CONFIGS[args.config]
+    storage = "float16" if args.variants.split(",")[0] == "fp16" else "float32"
+    prob = workloads.channel_problem(shape=shape, steps=args.forward_steps, collision=coll, storage=storage,
+                                     mrt_bulk_rate=bulk)
+    s = LbmSolver(normalize(prob))
+    raw = workloads.uniform_design(shape, 0) if dkind == "uniform" else workloads.sphere_design(shape, 0)
+    s.set_design(raw)
+    d = s.forward()
+    try:
+        s.gradient(workloads.objective_weights(), mode="steady", tolerance=1e-30, lambda_storage=storage,
+                   max_iterations=args.adjoint_iterations, check_every=args.adjoint_iterations)
+    except ConvergenceError:
+        pass
+    print(json.dumps({"profile_case": args.config, "storage": storage, "forward_steps": args.forward_steps,
+                      "adjoint_iterations": args.adjoint_iterations, "forward_ms": d.device_ms}))
+
+
 def cpu_sample(config, seconds_target=15.0, threads=None):
     """Oracle (FP64 CPU) forward + transposed steps on the same workload."""
     from implexity_b200 import normalize, workloads
@@ -301,7 +326,13 @@ def main():
     ap.add_argument("--config", default="channel128_trt", choices=sorted(CONFIGS))
     ap.add_argument("--variants", default="fp32,fp16")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--profile", action="store_true", help="run a short case of the bench kernels for ncu")
+    ap.add_argument("--forward-steps", type=int, default=20)
+    ap.add_argument("--adjoint-iterations", type=int, default=20)
     args = ap.parse_args()
+    if args.profile:
+        run_profile_case(args)
+        return
     rank, world, local = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), 0
     metric = "MLUPS fwd+adjoint D3Q19, FP32 vs FP16-store at grad err<1e-3; % HBM roofline"
     shape, T, coll, bulk, _ = CONFIGS[args.config]

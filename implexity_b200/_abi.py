@@ -36,6 +36,7 @@ EXPORTS = [
     "lbm_set_populations",
     "lbm_get_populations",
     "lbm_advance",
+    "lbm_trajectory",
     "lbm_responses",
     "lbm_fields",
     "lbm_gradient",
@@ -157,6 +158,7 @@ def _declare(lib: C.CDLL) -> None:
     lib.lbm_set_populations.argtypes = [h, _dp, C.c_size_t]
     lib.lbm_get_populations.argtypes = [h, _dp, C.c_size_t]
     lib.lbm_advance.argtypes = [h, C.c_int64, C.POINTER(Diag)]
+    lib.lbm_trajectory.argtypes = [h, _dp, _dp, _dp, _dp, C.c_size_t]
     lib.lbm_responses.argtypes = [h, _dp]
     lib.lbm_fields.argtypes = [h, _dp, _dp, _dp]
     lib.lbm_gradient.argtypes = [h, _dp, C.POINTER(AdjointOpts), _dp, C.POINTER(AdjointReport)]

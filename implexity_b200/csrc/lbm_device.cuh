@@ -1,0 +1,925 @@
+// lbm_device.cuh -- device building blocks shared by the sm_100a kernels
+// (lbm_forward.cu, lbm_adjoint.cu, lbm_misc.cu): storage conversions, AA-pattern
+// addressing, port maps, the collision and its transpose, compensated
+// reductions, and launch helpers.
+//
+// Memory layout (all on one GPU):
+//   populations  Q planes of n cells, plane q at pop + q*n; cells in the
+//                reference Grid order (i*ny + j)*nz + k, so axis 2 is the
+//                contiguous one.  FP32 stores g = f - w; FP16/BF16 store g/w.
+//   mask         one uint32 per cell (lbm_common.cuh)
+//   alpha, phi   FP32 per cell
+//   lambda       Q planes, adjoint populations (FP32/FP16/BF16, global scale)
+//   record       4 FP32 planes (rho-1, u) of the forward state the adjoint
+//                linearises at
+//
+// Streaming is the AA pattern: one population array updated in place.  A step
+// of parity 0 reads a cell's own slots and writes its post-collision values
+// into the opposite slots of the same cell; a step of parity 1 reads the
+// neighbours' opposite slots (the post-collision values streaming in) and
+// writes to the neighbours' slots.  A blocked link (halfway bounce-back,
+// Streaming::new solver.rs:84-119) reads/writes the cell's own slot instead.
+// Every slot is read and written by exactly one thread per step, so the
+// update is race free without a second buffer.  The adjoint transposes the
+// same pattern: the AA scheme run with the velocities reversed (pull from
+// x + c_q), linearised at a recorded (rho, u).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <mutex>
+#include <unordered_map>
+
+#include "lbm_launch.h"
+#include "lbm_tma.cuh"
+
+namespace lbm {
+namespace {
+
+constexpr int BLOCK = 256;
+constexpr unsigned FULL = 0xffffffffu;
+
+// ------------------------------------------------------------------ storage
+template <typename T>
+struct Cvt;
+template <>
+struct Cvt<float> {
+    static constexpr bool scaled = false;
+    __device__ __forceinline__ static float to(float v) { return v; }
+    __device__ __forceinline__ static float from(float v) { return v; }
+};
+template <>
+struct Cvt<__half> {
+    static constexpr bool scaled = true;
+    __device__ __forceinline__ static float to(__half v) { return __half2float(v); }
+    __device__ __forceinline__ static __half from(float v) { return __float2half_rn(v); }
+};
+template <>
+struct Cvt<__nv_bfloat16> {
+    static constexpr bool scaled = true;
+    __device__ __forceinline__ static float to(__nv_bfloat16 v) { return __bfloat162float(v); }
+    __device__ __forceinline__ static __nv_bfloat16 from(float v) { return __float2bfloat16_rn(v); }
+};
+
+// Stochastic rounding to the 16-bit formats: add uniform random bits below
+// the kept mantissa, then truncate.  A nearly steady state is re-rounded
+// every step; with round-to-nearest the same rounding errors repeat and the
+// mass drifts linearly in time, with stochastic rounding they average out.
+template <typename T>
+__device__ __forceinline__ T round_stochastic(float v, uint32_t r);
+template <>
+__device__ __forceinline__ __half round_stochastic<__half>(float v, uint32_t r) {
+    return __float2half_rz(__uint_as_float(__float_as_uint(v) + (r >> 19)));  // 13 dropped bits
+}
+template <>
+__device__ __forceinline__ __nv_bfloat16 round_stochastic<__nv_bfloat16>(float v, uint32_t r) {
+    return __float2bfloat16_rz(__uint_as_float(__float_as_uint(v) + (r >> 16)));  // 16 dropped bits
+}
+
+// Per-cell random stream: one integer hash of (cell, absolute step), then an
+// LCG step per stored value (its high bits feed the rounding).  Deterministic,
+// so recomputation from a checkpoint reproduces the stored states exactly.
+__device__ __forceinline__ uint32_t cell_seed(uint32_t x, uint32_t step) {
+    uint32_t h = x * 0x9E3779B1u ^ (step + 0x632BE5ABu) * 0x85EBCA77u;
+    h ^= h >> 16;
+    h *= 0x7FEB352Du;
+    h ^= h >> 15;
+    h *= 0x846CA68Bu;
+    h ^= h >> 16;
+    return h;
+}
+__device__ __forceinline__ uint32_t lcg(uint32_t& s) {
+    s = s * 1664525u + 1013904223u;
+    return s;
+}
+
+// population value of direction q (g = f - w) <-> stored element
+template <int Q, typename T>
+__device__ __forceinline__ float pdec(T v, int q) {
+    if constexpr (Cvt<T>::scaled) return Cvt<T>::to(v) * Lat<Q>::w(q);
+    else return Cvt<T>::to(v);
+}
+template <int Q, typename T>
+__device__ __forceinline__ T penc(float g, int q) {
+    if constexpr (Cvt<T>::scaled) return Cvt<T>::from(g * (float)(1.0 / Lat<Q>::wd(q)));
+    else return Cvt<T>::from(g);
+}
+template <int Q, typename T>
+__device__ __forceinline__ T penc_sr(float g, int q, uint32_t& rs) {
+    if constexpr (Cvt<T>::scaled) return round_stochastic<T>(g * (float)(1.0 / Lat<Q>::wd(q)), lcg(rs));
+    else return Cvt<T>::from(g);
+}
+
+// ------------------------------------------------------------------ indexing
+// All population indices q*n + x fit in 32 bits (the runtime checks
+// Q*n < 2^32), which keeps the per-direction address arithmetic in 32-bit
+// integer units.
+__device__ __forceinline__ uint32_t neighbor(const Geometry& G, uint32_t x, uint32_t m, int dx, int dy, int dz) {
+    if (!(m & MASK_WRAP)) return x + (uint32_t)(dx * (int)G.sx + dy * (int)G.sy + dz);
+    int k = (int)(x % (uint32_t)G.nz);
+    uint32_t ij = x / (uint32_t)G.nz;
+    int j = (int)(ij % (uint32_t)G.ny);
+    int i = (int)(ij / (uint32_t)G.ny);
+    i += dx;
+    j += dy;
+    k += dz;
+    if (i < 0) i += G.nx;
+    else if (i >= G.nx) i -= G.nx;
+    if (j < 0) j += G.ny;
+    else if (j >= G.ny) j -= G.ny;
+    if (k < 0) k += G.nz;
+    else if (k >= G.nz) k -= G.nz;
+    return ((uint32_t)i * (uint32_t)G.ny + (uint32_t)j) * (uint32_t)G.nz + (uint32_t)k;
+}
+
+__device__ __forceinline__ void coords(const Geometry& G, int64_t x, int64_t& i, int64_t& j, int64_t& k) {
+    k = x % G.nz;
+    int64_t ij = x / G.nz;
+    j = ij % G.ny;
+    i = ij / G.ny;
+}
+
+// Forward AA access.  parity 0 reads own slots; parity 1 gathers the
+// neighbours' opposite slots (own slot when the link is blocked).
+// Linear offset of the neighbour x + c (no wrap): a constant per direction.
+template <int Q>
+__device__ __forceinline__ uint32_t lin(const Geometry& G, int q, int sign) {
+    using L = Lat<Q>;
+    return (uint32_t)(sign * (L::cx(q) * (int)G.sx + L::cy(q) * (int)G.sy + L::cz(q)));
+}
+
+// Forward AA access of the stored elements of one cell.  parity 0 reads the
+// cell's own slots; parity 1 gathers the neighbours' opposite slots (own slot
+// when the link is blocked).  Cells away from periodic faces take the fast
+// path: a select between two addresses per direction, no branches.
+template <int Q, typename T>
+__device__ __forceinline__ void load_raw(const T* __restrict__ A, const Geometry& G, uint32_t x, uint32_t m,
+                                         int parity, T (&r)[Q]) {
+    using L = Lat<Q>;
+    const uint32_t n = (uint32_t)G.n;
+    if (parity == 0) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) r[q] = A[q * n + x];
+    } else if (!(m & MASK_WRAP)) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const uint32_t own = q * n + x;
+            const uint32_t nb = opp<Q>(q) * n + x + lin<Q>(G, q, -1);
+            r[q] = A[((m >> q) & 1u) ? own : nb];
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            uint32_t idx;
+            if (m & (1u << q)) idx = q * n + x;
+            else idx = opp<Q>(q) * n + neighbor(G, x, m, -L::cx(q), -L::cy(q), -L::cz(q));
+            r[q] = A[idx];
+        }
+    }
+}
+
+template <int Q, typename T>
+__device__ __forceinline__ void decode(const T (&r)[Q], float (&g)[Q]) {
+#pragma unroll
+    for (int q = 0; q < Q; ++q) g[q] = pdec<Q, T>(r[q], q);
+}
+
+template <int Q, typename T>
+__device__ __forceinline__ void load_pop(const T* __restrict__ A, const Geometry& G, uint32_t x, uint32_t m,
+                                         int parity, float (&g)[Q]) {
+    T r[Q];
+    load_raw<Q, T>(A, G, x, m, parity, r);
+    decode<Q, T>(r, g);
+}
+
+template <int Q, typename T>
+__device__ __forceinline__ void store_pop(T* A, const Geometry& G, uint32_t x, uint32_t m, int parity,
+                                          const float (&g)[Q], uint32_t step) {
+    using L = Lat<Q>;
+    const uint32_t n = (uint32_t)G.n;
+    uint32_t rs = 0;
+    if constexpr (Cvt<T>::scaled) rs = cell_seed(x, step);
+    if (parity == 0) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) A[opp<Q>(q) * n + x] = penc_sr<Q, T>(g[q], q, rs);
+    } else if (!(m & MASK_WRAP)) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            // x + c_q a wall or solid: bounce back into the own opposite slot
+            const uint32_t own = opp<Q>(q) * n + x;
+            const uint32_t nb = q * n + x + lin<Q>(G, q, +1);
+            A[((m >> opp<Q>(q)) & 1u) ? own : nb] = penc_sr<Q, T>(g[q], q, rs);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            uint32_t idx;
+            if (m & (1u << opp<Q>(q))) idx = opp<Q>(q) * n + x;
+            else idx = q * n + neighbor(G, x, m, L::cx(q), L::cy(q), L::cz(q));
+            A[idx] = penc_sr<Q, T>(g[q], q, rs);
+        }
+    }
+}
+
+// Adjoint AA access (velocities reversed).
+template <int Q, typename T>
+__device__ __forceinline__ void load_lam_raw(const T* __restrict__ B, const Geometry& G, uint32_t x, uint32_t m,
+                                             int parity, T (&r)[Q]) {
+    using L = Lat<Q>;
+    const uint32_t n = (uint32_t)G.n;
+    if (parity == 0) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) r[q] = B[q * n + x];
+    } else if (!(m & MASK_WRAP)) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const uint32_t own = q * n + x;
+            const uint32_t nb = opp<Q>(q) * n + x + lin<Q>(G, q, +1);
+            r[q] = B[((m >> opp<Q>(q)) & 1u) ? own : nb];
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            uint32_t idx;
+            if (m & (1u << opp<Q>(q))) idx = q * n + x;
+            else idx = opp<Q>(q) * n + neighbor(G, x, m, L::cx(q), L::cy(q), L::cz(q));
+            r[q] = B[idx];
+        }
+    }
+}
+
+template <int Q, typename T>
+__device__ __forceinline__ void load_lam(const T* __restrict__ B, const Geometry& G, uint32_t x, uint32_t m,
+                                         int parity, float scale, float (&v)[Q]) {
+    T r[Q];
+    load_lam_raw<Q, T>(B, G, x, m, parity, r);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(r[q]) * scale;
+}
+
+template <int Q, typename T>
+__device__ __forceinline__ void store_lam(T* B, const Geometry& G, uint32_t x, uint32_t m, int parity, float scale,
+                                          const float (&v)[Q]) {
+    using L = Lat<Q>;
+    const uint32_t n = (uint32_t)G.n;
+    if (parity == 0) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) B[opp<Q>(q) * n + x] = Cvt<T>::from(v[q] * scale);
+    } else if (!(m & MASK_WRAP)) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const uint32_t own = opp<Q>(q) * n + x;
+            const uint32_t nb = q * n + x + lin<Q>(G, q, -1);
+            B[((m >> q) & 1u) ? own : nb] = Cvt<T>::from(v[q] * scale);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            uint32_t idx;
+            if (m & (1u << q)) idx = opp<Q>(q) * n + x;
+            else idx = q * n + neighbor(G, x, m, -L::cx(q), -L::cy(q), -L::cz(q));
+            B[idx] = Cvt<T>::from(v[q] * scale);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ ports
+// Applies the affine port map to a port cell's streamed populations; returns
+// the exchanged mass (ports.rs:560-579).
+template <int Q>
+__device__ __forceinline__ float apply_port(const PortMap& P, float (&g)[Q]) {
+    float in[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) in[q] = g[q];
+    float exch = 0.f;
+    const uint32_t um = P.unknown_mask;
+#pragma unroll
+    for (int r = 0; r < Q; ++r) {
+        if (um & (1u << r)) {
+            float acc = P.bias[r];
+#pragma unroll
+            for (int k = 0; k < Q; ++k) acc = fmaf(P.jac[r][k], in[k], acc);
+            exch += acc - in[r];
+            g[r] = acc;
+        }
+    }
+    return exch;
+}
+
+// lambda <- J^T lambda for a port cell (apply_ports_vjp, ports.rs:582-621).
+template <int Q>
+__device__ __forceinline__ void port_transpose(const PortMap& P, float (&v)[Q]) {
+    float in[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) in[q] = v[q];
+    const uint32_t um = P.unknown_mask;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        float acc = (um & (1u << k)) ? 0.f : in[k];
+#pragma unroll
+        for (int r = 0; r < Q; ++r)
+            if (um & (1u << r)) acc = fmaf(P.jac[r][k], in[r], acc);
+        v[k] = acc;
+    }
+}
+
+// ------------------------------------------------------------------ physics
+struct Macro {
+    float rp, rho, u[3], F[3];
+};
+
+// Implicit half-step Brinkman velocity and Guo force (solver.rs:190-196,
+// moving/psm.rs:213-226 with zero solid velocity).
+template <int Q>
+__device__ __forceinline__ Macro macroscopic(const float (&g)[Q], float alpha, const Physics& P) {
+    using L = Lat<Q>;
+    Macro M;
+    float rp = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        rp += g[q];
+        if (L::cx(q)) jx += L::cx(q) * g[q];
+        if (L::cy(q)) jy += L::cy(q) * g[q];
+        if (L::cz(q)) jz += L::cz(q) * g[q];
+    }
+    M.rp = rp;
+    M.rho = 1.f + rp;
+    const float inv_s = 1.f / (1.f + 0.5f * alpha);
+    const float inv_rho = 1.f / M.rho;
+    M.u[0] = (jx * inv_rho + 0.5f * P.a[0]) * inv_s;
+    M.u[1] = (jy * inv_rho + 0.5f * P.a[1]) * inv_s;
+    M.u[2] = (jz * inv_rho + 0.5f * P.a[2]) * inv_s;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) M.F[d] = M.rho * (P.a[d] - alpha * M.u[d]);
+    return M;
+}
+
+template <int Q>
+__device__ __forceinline__ float dotc(int q, const float (&v)[3]) {
+    using L = Lat<Q>;
+    float s = 0.f;
+    if (L::cx(q)) s += L::cx(q) * v[0];
+    if (L::cy(q)) s += L::cy(q) * v[1];
+    if (L::cz(q)) s += L::cz(q) * v[2];
+    return s;
+}
+
+// TRT collision in pair form (moving/collision.rs:457-488), in shifted
+// variables g = f - w; BGK is the case om == omega.  MRT adds the rank-one
+// corrections of the moments whose rate differs from the shear rate: the
+// odd moments of the Gram-Schmidt basis span exactly the antisymmetric
+// subspace, so MRT with all even rates equal to omega is TRT.
+template <int Q, int COLL>
+__device__ __forceinline__ void collide(float (&g)[Q], const Macro& M, const Physics& P) {
+    using L = Lat<Q>;
+    const float om = P.omega, omm = P.om;
+    const float kp = 1.f - 0.5f * om, km = 1.f - 0.5f * omm;
+    const float* u = M.u;
+    const float* F = M.F;
+    const float usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const float uf = u[0] * F[0] + u[1] * F[1] + u[2] * F[2];
+    const float rho = M.rho, rp = M.rp;
+    float dproj[MAX_PROJ];
+    if constexpr (COLL == CK_MRT) {
+#pragma unroll
+        for (int p = 0; p < MAX_PROJ; ++p) dproj[p] = 0.f;
+    }
+    {
+        const float w0 = L::w(0);
+        const float geq = w0 * (rp - 1.5f * rho * usq);
+        const float src = -3.f * w0 * uf;
+        if constexpr (COLL == CK_MRT) {
+            const float y0 = g[0] - geq + 0.5f * src;
+#pragma unroll
+            for (int p = 0; p < MAX_PROJ; ++p)
+                if (p < P.n_proj) dproj[p] = fmaf(P.proj_right[p][0], y0, dproj[p]);
+        }
+        g[0] = g[0] - om * (g[0] - geq) + kp * src;
+    }
+#pragma unroll
+    for (int i = 1; i <= L::NPAIR; ++i) {
+        const int o = opp<Q>(i);
+        const float w = L::w(i);
+        const float cu = dotc<Q>(i, M.u);
+        const float cf = dotc<Q>(i, M.F);
+        const float geqp = w * (rp + rho * (4.5f * cu * cu - 1.5f * usq));
+        const float eqm = 3.f * rho * w * cu;
+        const float sp = w * (9.f * cu * cf - 3.f * uf);
+        const float sm = 3.f * w * cf;
+        const float gp = 0.5f * (g[i] + g[o]);
+        const float gm = 0.5f * (g[i] - g[o]);
+        if constexpr (COLL == CK_MRT) {
+            const float yp = gp - geqp + 0.5f * sp;
+#pragma unroll
+            for (int p = 0; p < MAX_PROJ; ++p)
+                if (p < P.n_proj) dproj[p] = fmaf(2.f * P.proj_right[p][i], yp, dproj[p]);
+        }
+        const float A = kp * sp - om * (gp - geqp);
+        const float Bv = km * sm - omm * (gm - eqm);
+        g[i] = g[i] + A + Bv;
+        g[o] = g[o] + A - Bv;
+    }
+    if constexpr (COLL == CK_MRT) {
+#pragma unroll
+        for (int p = 0; p < MAX_PROJ; ++p) {
+            if (p < P.n_proj) {
+                const float c = P.proj_rate[p] * dproj[p];
+#pragma unroll
+                for (int i = 0; i < Q; ++i) g[i] = fmaf(-c, P.proj_left[p][i], g[i]);
+            }
+        }
+    }
+    // The collision conserves mass exactly; the FP32 weights do not sum to one,
+    // which would leak (rho - 1) * (sum w - 1) per cell and step -- systematic
+    // where the pressure has one sign.  The rest population takes the
+    // remainder, so only unbiased rounding remains.
+    float moving = 0.f;
+#pragma unroll
+    for (int i = 1; i < Q; ++i) moving += g[i];
+    g[0] = rp - moving;
+}
+
+// Collision transpose at the recorded (rho, u): given gb = d(loss)/d(post),
+// returns d(loss)/d(f) in gb and d(loss)/d(alpha).  Derivation: post = f - R y
+// + src, y = f - eq(rho, u) + src(u, F)/2; the cotangents of eq and src only
+// need the weighted zeroth, first and second moments of R^T gb, then the
+// Brinkman chain F = rho (a - alpha u), u = (m/rho + a/2)/(1 + alpha/2).
+template <int Q, int COLL>
+__device__ __forceinline__ float collide_vjp(float (&gb)[Q], float rp, const float (&u)[3], float alpha,
+                                             const Physics& P) {
+    using L = Lat<Q>;
+    const float om = P.omega, omm = P.om;
+    const float rho = 1.f + rp;
+    const float s = 1.f + 0.5f * alpha;
+    float F[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) F[d] = rho * (P.a[d] - alpha * u[d]);
+    // z = R^T gb
+    float z[Q];
+    z[0] = om * gb[0];
+#pragma unroll
+    for (int i = 1; i <= L::NPAIR; ++i) {
+        const int o = opp<Q>(i);
+        const float p = 0.5f * (gb[i] + gb[o]), mm = 0.5f * (gb[i] - gb[o]);
+        z[i] = om * p + omm * mm;
+        z[o] = om * p - omm * mm;
+    }
+    if constexpr (COLL == CK_MRT) {
+#pragma unroll
+        for (int p = 0; p < MAX_PROJ; ++p) {
+            if (p < P.n_proj) {
+                float e = 0.f;
+#pragma unroll
+                for (int i = 0; i < Q; ++i) e = fmaf(P.proj_left[p][i], gb[i], e);
+                const float c = P.proj_rate[p] * e;
+#pragma unroll
+                for (int i = 0; i < Q; ++i) z[i] = fmaf(c, P.proj_right[p][i], z[i]);
+            }
+        }
+    }
+    // weighted moments of z and of h = gb - z/2
+    float Z0 = 0.f, Z1[3] = {0.f, 0.f, 0.f}, Z2[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float H0 = 0.f, H1[3] = {0.f, 0.f, 0.f}, H2[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const float w = L::w(i);
+        const float zw = w * z[i];
+        const float hw = w * (gb[i] - 0.5f * z[i]);
+        const int c0 = L::cx(i), c1 = L::cy(i), c2 = L::cz(i);
+        Z0 += zw;
+        H0 += hw;
+        if (c0) { Z1[0] += c0 * zw; H1[0] += c0 * hw; }
+        if (c1) { Z1[1] += c1 * zw; H1[1] += c1 * hw; }
+        if (c2) { Z1[2] += c2 * zw; H1[2] += c2 * hw; }
+        if (c0) { Z2[0] += zw; H2[0] += hw; }
+        if (c1) { Z2[1] += zw; H2[1] += hw; }
+        if (c2) { Z2[2] += zw; H2[2] += hw; }
+        if (c0 && c1) { Z2[3] += c0 * c1 * zw; H2[3] += c0 * c1 * hw; }
+        if (c0 && c2) { Z2[4] += c0 * c2 * zw; H2[4] += c0 * c2 * hw; }
+        if (c1 && c2) { Z2[5] += c1 * c2 * zw; H2[5] += c1 * c2 * hw; }
+    }
+    // Z2 u, H2 u, H2 F (symmetric 3x3 stored xx yy zz xy xz yz)
+    auto mul = [](const float (&S)[6], const float* v, float* out) {
+        out[0] = S[0] * v[0] + S[3] * v[1] + S[4] * v[2];
+        out[1] = S[3] * v[0] + S[1] * v[1] + S[5] * v[2];
+        out[2] = S[4] * v[0] + S[5] * v[1] + S[2] * v[2];
+    };
+    float Z2u[3], H2u[3], H2F[3];
+    mul(Z2, u, Z2u);
+    mul(H2, u, H2u);
+    mul(H2, F, H2F);
+    const float usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    float rho_bar = Z0 * (1.f - 1.5f * usq) + 3.f * (u[0] * Z1[0] + u[1] * Z1[1] + u[2] * Z1[2]) +
+                    4.5f * (u[0] * Z2u[0] + u[1] * Z2u[1] + u[2] * Z2u[2]);
+    float ub[3], Fb[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        ub[d] = rho * (3.f * Z1[d] + 9.f * Z2u[d] - 3.f * u[d] * Z0) + 9.f * H2F[d] - 3.f * F[d] * H0;
+        Fb[d] = 3.f * H1[d] + 9.f * H2u[d] - 3.f * u[d] * H0;
+    }
+    float abar = 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        rho_bar += Fb[d] * (P.a[d] - alpha * u[d]);
+        abar -= rho * Fb[d] * u[d];
+        ub[d] -= rho * alpha * Fb[d];
+    }
+    const float inv = 1.f / (s * rho);
+    float mb[3];
+    float sbar = 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        mb[d] = ub[d] * inv;
+        rho_bar -= ub[d] * (s * u[d] - 0.5f * P.a[d]) * inv;
+        sbar -= ub[d] * u[d] / s;
+    }
+    abar += 0.5f * sbar;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        float v = gb[i] - z[i] + rho_bar;
+        if (L::cx(i)) v += L::cx(i) * mb[0];
+        if (L::cy(i)) v += L::cy(i) * mb[1];
+        if (L::cz(i)) v += L::cz(i) * mb[2];
+        gb[i] = v;
+    }
+    return abar;
+}
+
+// ------------------------------------------------------------------ reductions
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+    s = a + b;
+    double bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+// (h, l) += (h2, l2), compensated
+__device__ __forceinline__ void dd_add(double& h, double& l, double h2, double l2) {
+    double s, e;
+    two_sum(h, h2, s, e);
+    e += l + l2;
+    h = s + e;
+    l = e - (h - s);
+}
+
+// Per-thread admission accumulators (a thread sees a few tens of cells, so
+// single precision partial sums are exact to ~1e-7 of their own size; the
+// block and grid reductions are compensated double).
+struct DiagLocal {
+    float mass, exch, minf, maxu2;
+    int nf;
+    __device__ void init() {
+        mass = exch = 0.f;
+        minf = INFINITY;
+        maxu2 = 0.f;
+        nf = 0;
+    }
+};
+
+struct DiagAcc {
+    double mh, ml, eh, el;
+    float minf, maxu2;
+    int nf;
+    __device__ void init() {
+        mh = ml = eh = el = 0.0;
+        minf = INFINITY;
+        maxu2 = 0.f;
+        nf = 0;
+    }
+    __device__ void merge(const DiagAcc& o) {
+        dd_add(mh, ml, o.mh, o.ml);
+        dd_add(eh, el, o.eh, o.el);
+        minf = fminf(minf, o.minf);
+        maxu2 = fmaxf(maxu2, o.maxu2);
+        nf |= o.nf;
+    }
+    __device__ void shfl_merge(int off) {
+        DiagAcc o;
+        o.mh = __shfl_down_sync(FULL, mh, off);
+        o.ml = __shfl_down_sync(FULL, ml, off);
+        o.eh = __shfl_down_sync(FULL, eh, off);
+        o.el = __shfl_down_sync(FULL, el, off);
+        o.minf = __shfl_down_sync(FULL, minf, off);
+        o.maxu2 = __shfl_down_sync(FULL, maxu2, off);
+        o.nf = __shfl_down_sync(FULL, nf, off);
+        merge(o);
+    }
+};
+
+__device__ DiagAcc block_reduce(DiagAcc v) {
+    __shared__ DiagAcc sh[32];
+    for (int off = 16; off > 0; off >>= 1) v.shfl_merge(off);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        if (lane < (int)(blockDim.x >> 5)) v = sh[lane];
+        else v.init();
+        for (int off = 16; off > 0; off >>= 1) v.shfl_merge(off);
+    }
+    return v;
+}
+
+// Writes one block's partial, and lets the last block to finish combine all
+// partials in a fixed order (deterministic) into *out.  No block waits.
+__device__ void finish_diag(const DiagLocal& loc, StepDiag* out, const Reduce& red) {
+    __shared__ bool last;
+    DiagAcc v;
+    v.mh = loc.mass;
+    v.ml = 0.0;
+    v.eh = loc.exch;
+    v.el = 0.0;
+    v.minf = loc.minf;
+    v.maxu2 = loc.maxu2;
+    v.nf = loc.nf;
+    v = block_reduce(v);
+    if (threadIdx.x == 0) {
+        double* p = red.partial + (size_t)blockIdx.x * 8;
+        p[0] = v.mh;
+        p[1] = v.ml;
+        p[2] = v.eh;
+        p[3] = v.el;
+        p[4] = v.minf;
+        p[5] = v.maxu2;
+        p[6] = v.nf;
+        __threadfence();
+        unsigned t = atomicAdd(red.counter, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    DiagAcc acc;
+    acc.init();
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+        const double* p = red.partial + (size_t)b * 8;
+        DiagAcc o;
+        o.mh = __ldcg(p + 0);
+        o.ml = __ldcg(p + 1);
+        o.eh = __ldcg(p + 2);
+        o.el = __ldcg(p + 3);
+        o.minf = (float)__ldcg(p + 4);
+        o.maxu2 = (float)__ldcg(p + 5);
+        o.nf = (int)__ldcg(p + 6);
+        acc.merge(o);
+    }
+    acc = block_reduce(acc);
+    if (threadIdx.x == 0) {
+        out->mass_hi = acc.mh;
+        out->mass_lo = acc.ml;
+        out->exch_hi = acc.eh;
+        out->exch_lo = acc.el;
+        out->min_f = acc.minf;
+        out->max_u2 = acc.maxu2;
+        out->nonfinite = acc.nf;
+        *red.counter = 0;
+        __threadfence();
+    }
+}
+
+// NS compensated double sums.
+template <int NS>
+struct Sums {
+    double h[NS], l[NS];
+    __device__ void init() {
+#pragma unroll
+        for (int k = 0; k < NS; ++k) h[k] = l[k] = 0.0;
+    }
+    __device__ void add(int k, double v) { dd_add(h[k], l[k], v, 0.0); }
+    __device__ void merge(const Sums& o) {
+#pragma unroll
+        for (int k = 0; k < NS; ++k) dd_add(h[k], l[k], o.h[k], o.l[k]);
+    }
+    __device__ void shfl_merge(int off) {
+        Sums o;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+            o.h[k] = __shfl_down_sync(FULL, h[k], off);
+            o.l[k] = __shfl_down_sync(FULL, l[k], off);
+        }
+        merge(o);
+    }
+};
+
+template <int NS>
+__device__ Sums<NS> block_reduce_sums(Sums<NS> v) {
+    __shared__ Sums<NS> sh[32];
+    for (int off = 16; off > 0; off >>= 1) v.shfl_merge(off);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        if (lane < (int)(blockDim.x >> 5)) v = sh[lane];
+        else v.init();
+        for (int off = 16; off > 0; off >>= 1) v.shfl_merge(off);
+    }
+    return v;
+}
+
+template <int NS>
+__device__ void finish_sums(Sums<NS> v, double* out, const Reduce& red) {
+    __shared__ bool last;
+    v = block_reduce_sums<NS>(v);
+    if (threadIdx.x == 0) {
+        double* p = red.partial + (size_t)blockIdx.x * 2 * NS;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+            p[2 * k] = v.h[k];
+            p[2 * k + 1] = v.l[k];
+        }
+        __threadfence();
+        unsigned t = atomicAdd(red.counter, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    Sums<NS> acc;
+    acc.init();
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+        const double* p = red.partial + (size_t)b * 2 * NS;
+        Sums<NS> o;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+            o.h[k] = __ldcg(p + 2 * k);
+            o.l[k] = __ldcg(p + 2 * k + 1);
+        }
+        acc.merge(o);
+    }
+    acc = block_reduce_sums<NS>(acc);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+            out[2 * k] = acc.h[k];
+            out[2 * k + 1] = acc.l[k];
+        }
+        *red.counter = 0;
+        __threadfence();
+    }
+}
+
+
+// ------------------------------------------------------------------ launch helpers
+#define LBM_STORAGE_DISPATCH(storage, T, ...)            \
+    switch (storage) {                                   \
+        case ST_F32: {                                   \
+            using T = float;                             \
+            __VA_ARGS__;                                 \
+            break;                                       \
+        }                                                \
+        case ST_F16: {                                   \
+            using T = __half;                            \
+            __VA_ARGS__;                                 \
+            break;                                       \
+        }                                                \
+        default: {                                       \
+            using T = __nv_bfloat16;                     \
+            __VA_ARGS__;                                 \
+            break;                                       \
+        }                                                \
+    }
+
+[[maybe_unused]] static int blocks_for(int64_t n, int cap, int tile = BLOCK) {
+    int64_t b = (n + tile - 1) / tile;
+    if (cap > 0 && b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
+}
+
+// One wave of resident blocks (occupancy of this exact kernel x SM count);
+// the grid-stride loops then give every thread the same number of cells.
+[[maybe_unused]] static int persistent_grid(const void* kernel, int64_t n, size_t smem = 0, int threads = BLOCK, int tile = BLOCK) {
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> per_sm;
+    [[maybe_unused]] static int sms = 0;
+    int b;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (sms == 0) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (sms <= 0) sms = 148;
+        }
+        auto it = per_sm.find(kernel);
+        if (it == per_sm.end()) {
+            int nb = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem) != cudaSuccess || nb <= 0) nb = 1;
+            it = per_sm.emplace(kernel, nb).first;
+        }
+        b = it->second * sms;
+    }
+    return blocks_for(n, b, tile);
+}
+
+
+}  // namespace
+}  // namespace lbm
+
+namespace lbm {
+namespace {
+
+// ------------------------------------------------------------------ staged pipelines
+// A tile is TILE consecutive cells.  For every direction the AA access of a
+// whole tile is one contiguous run of a population plane: the cells' own
+// slots (parity 0) or the run shifted by the direction's constant linear
+// offset (parity 1).  A producer warp issues one bulk copy per run into a
+// ring of STAGES shared-memory buffers (cp.async.bulk completing on a "full"
+// mbarrier); eight consumer warps compute one cell each and release the
+// buffer on an "empty" mbarrier.  Runs are fetched 16-byte aligned and one
+// vector longer than the tile; each consumer indexes its element with the
+// run's misalignment.  Blocked links (walls, solids) and cells on periodic
+// faces read their few populations from global memory directly.
+constexpr int CONSUMER_WARPS = 8;
+constexpr int TILE = CONSUMER_WARPS * 32;
+constexpr int TPB = TILE + 32;
+constexpr int STAGES = 3;
+
+template <typename T>
+struct Vec16 {
+    static constexpr int V = 16 / (int)sizeof(T);  // elements per 16 bytes
+    static constexpr int RUN = TILE + V;            // elements per staged run
+    static constexpr int BYTES = RUN * (int)sizeof(T);
+};
+constexpr int FRUN = TILE + 4;  // float / uint32 runs (mask, alpha, record)
+constexpr int FRUN_BYTES = FRUN * 4;
+
+template <typename S>
+__host__ __device__ constexpr size_t stage_stride() {
+    return (sizeof(S) + 127) / 128 * 128;
+}
+template <typename S>
+__host__ __device__ constexpr size_t pipe_bytes() {
+    return 128 + STAGES * stage_stride<S>();
+}
+template <typename S>
+__device__ __forceinline__ S* stage_at(unsigned char* smem, int s) {
+    return reinterpret_cast<S*>(smem + 128 + s * stage_stride<S>());
+}
+
+// Forward AA store with the parity known at compile time.
+template <int Q, typename T, int PAR>
+__device__ __forceinline__ void store_pop_p(T* A, const Geometry& G, uint32_t x, uint32_t m, const float (&g)[Q],
+                                            uint32_t step) {
+    using L = Lat<Q>;
+    const uint32_t n = (uint32_t)G.n;
+    uint32_t rs = 0;
+    if constexpr (Cvt<T>::scaled) rs = cell_seed(x, step);
+    if constexpr (PAR == 0) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) A[opp<Q>(q) * n + x] = penc_sr<Q, T>(g[q], q, rs);
+    } else {
+        if (!(m & MASK_WRAP)) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const uint32_t own = opp<Q>(q) * n + x;
+                const uint32_t nb = q * n + x + lin<Q>(G, q, +1);
+                A[((m >> opp<Q>(q)) & 1u) ? own : nb] = penc_sr<Q, T>(g[q], q, rs);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                uint32_t idx;
+                if (m & (1u << opp<Q>(q))) idx = opp<Q>(q) * n + x;
+                else idx = q * n + neighbor(G, x, m, L::cx(q), L::cy(q), L::cz(q));
+                A[idx] = penc_sr<Q, T>(g[q], q, rs);
+            }
+        }
+    }
+}
+
+template <int Q, typename T, int PAR>
+__device__ __forceinline__ void store_lam_p(T* B, const Geometry& G, uint32_t x, uint32_t m, float scale,
+                                            const float (&v)[Q]) {
+    using L = Lat<Q>;
+    const uint32_t n = (uint32_t)G.n;
+    if constexpr (PAR == 0) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) B[opp<Q>(q) * n + x] = Cvt<T>::from(v[q] * scale);
+    } else {
+        if (!(m & MASK_WRAP)) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const uint32_t own = opp<Q>(q) * n + x;
+                const uint32_t nb = q * n + x + lin<Q>(G, q, -1);
+                B[((m >> q) & 1u) ? own : nb] = Cvt<T>::from(v[q] * scale);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                uint32_t idx;
+                if (m & (1u << q)) idx = opp<Q>(q) * n + x;
+                else idx = q * n + neighbor(G, x, m, -L::cx(q), -L::cy(q), -L::cz(q));
+                B[idx] = Cvt<T>::from(v[q] * scale);
+            }
+        }
+    }
+}
+
+template <typename K>
+cudaError_t set_smem(K kernel, size_t bytes) {
+    return cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+}  // namespace
+}  // namespace lbm

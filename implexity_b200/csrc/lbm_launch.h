@@ -8,7 +8,13 @@
 
 namespace lbm {
 
-// Population storage.  F32 stores g = f - w; F16/BF16 store g/w.
+// Population storage.  F32 stores g = f - w; F16/BF16 store g/w.  Population
+// and adjoint arrays carry pop_pad(G) elements of padding before plane 0 and
+// after the last plane (the staged runs of the stepping kernels read a little
+// outside the planes); per-cell float/uint arrays carry CELL_PAD elements
+// after the last cell.
+constexpr int64_t CELL_PAD = 1024;
+inline int64_t pop_pad(const Geometry& G) { return ((G.sx + G.sy + 1 + 2 * CELL_PAD) + 63) / 64 * 64; }
 enum StoreKind { ST_F32 = 0, ST_F16 = 1, ST_BF16 = 2 };
 enum CollKind { CK_PAIRS = 0, CK_MRT = 1 };  // BGK runs as PAIRS with om == omega
 
@@ -25,6 +31,13 @@ struct FwdArgs {
     Reduce red;
     float* record;           // (rho-1, ux, uy, uz) planes (nullptr: off)
     int32_t collide;         // 0: only load/diag/record (no collision, no store)
+    uint32_t step;           // absolute step index (seeds the stochastic rounding)
+    int* err;                // set when a bounded wait gave up
+    // staged runs of this step's parity: element offset of each direction's
+    // 16-byte aligned run for the tile at x0 = 0, and the offset of the
+    // tile's first element inside it
+    int64_t run0[27];
+    int32_t rund[27];
 };
 
 struct AdjArgs {
@@ -44,6 +57,11 @@ struct AdjArgs {
     float abar_factor;       // abar += factor * d(loss)/d(alpha)
     double* norm2;           // sum of squares of the stored lambda (true units * out_scale), nullptr: off
     Reduce red;
+    int* err;                // set when a bounded wait gave up
+    int64_t run0[27];        // staged adjoint runs (see FwdArgs)
+    int32_t rund[27];
+    int64_t rec0[4];         // staged record runs
+    int32_t recd[4];
 };
 
 struct ObjArgs {
@@ -96,6 +114,11 @@ struct DesignArgs {
     float* scale;
     float* grad;
 };
+
+// Fills run0/rund for a tile-staged kernel: direction q's run starts at the
+// first used element q*n + x0 (parity 0) or opp(q)*n + x0 + dir*lin(q)
+// (parity 1), aligned down to `vec` elements.
+void run_table(int Q, const Geometry& G, int parity, int dir, int vec, int64_t* run0, int32_t* rund);
 
 cudaError_t launch_init(int Q, int storage, const Geometry& G, const Physics& P, void* pop, const uint32_t* mask,
                         cudaStream_t s);

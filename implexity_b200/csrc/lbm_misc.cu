@@ -1,0 +1,467 @@
+// lbm_misc.cu -- one-off kernels around the stepping: initial state,
+// responses and their VJP (the adjoint seed), state/adjoint layout
+// conversions, the design map and its transpose.
+#include "lbm_device.cuh"
+
+namespace lbm {
+namespace {
+
+// ------------------------------------------------------------------ kernels
+template <int Q, typename T>
+__global__ void __launch_bounds__(BLOCK) k_init(Geometry G, Physics P, T* A, const uint32_t* __restrict__ mask) {
+    using L = Lat<Q>;
+    for (int64_t x = (int64_t)blockIdx.x * BLOCK + threadIdx.x; x < G.n; x += (int64_t)gridDim.x * BLOCK) {
+        const bool solid = mask[x] & MASK_SOLID;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            // initial_populations, solver.rs:593-601: fluid w(1 - 1.5 c.a), solid w
+            const float ca = L::cx(q) * P.a[0] + L::cy(q) * P.a[1] + L::cz(q) * P.a[2];
+            const float g = solid ? 0.f : -1.5f * L::w(q) * ca;
+            A[(int64_t)q * G.n + x] = penc<Q, T>(g, q);
+        }
+    }
+}
+
+// Responses of one state (mode 0) or their VJP seeding the adjoint (mode 1).
+// vector_cell / vector_vjp, solver.rs:835-947, plus the pressure drop and the
+// viscous dissipation sigma:sigma / (2 rho nu) with the Guo-corrected
+// non-equilibrium stress sigma = -(1 - omega/2) (Pi_neq + (uF + Fu)/2).
+template <int Q, typename T, typename TL, int MODE>
+__global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
+    using L = Lat<Q>;
+    const T* A = static_cast<const T*>(a.pop);
+    const int64_t n = a.G.n;
+    Sums<8> acc;
+    acc.init();
+    double nsum = 0.0;
+    const float k = 1.f - 0.5f / a.tau;
+    const float nu = (a.tau - 0.5f) / 3.f;
+    for (uint32_t x = blockIdx.x * BLOCK + threadIdx.x; x < (uint32_t)n; x += gridDim.x * BLOCK) {
+        const uint32_t m = a.mask[x];
+        if (m & MASK_SOLID) {
+            if constexpr (MODE == 0) acc.add(5, (double)a.phi[x]);
+            else {
+                a.phibar[x] = (float)a.w[5];
+                a.abar_final[x] = 0.f;
+            }
+            continue;
+        }
+        float g[Q];
+        load_pop<Q, T>(A, a.G, x, m, a.parity, g);
+        const PortMap* pm = (m & MASK_PORT) ? &a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1] : nullptr;
+        if (a.apply_ports && pm) apply_port<Q>(*pm, g);
+        const float alpha = a.alpha[x];
+        Macro M = macroscopic<Q>(g, alpha, a.P);
+        // second moments of g: M2_ab = sum c_a c_b g (f adds delta/3)
+        float S[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int c0 = L::cx(q), c1 = L::cy(q), c2 = L::cz(q);
+            if (c0) S[0] += g[q];
+            if (c1) S[1] += g[q];
+            if (c2) S[2] += g[q];
+            if (c0 && c1) S[3] += c0 * c1 * g[q];
+            if (c0 && c2) S[4] += c0 * c2 * g[q];
+            if (c1 && c2) S[5] += c1 * c2 * g[q];
+        }
+        const float* u = M.u;
+        const float* F = M.F;
+        const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+        float sig[6];
+        float ss = 0.f;
+#pragma unroll
+        for (int e = 0; e < 6; ++e) {
+            const float pi = S[e] - (e < 3 ? M.rp / 3.f : 0.f) - M.rho * u[ia[e]] * u[ib[e]];
+            const float t = 0.5f * (u[ia[e]] * F[ib[e]] + u[ib[e]] * F[ia[e]]);
+            sig[e] = -k * (pi + t);
+            ss += (e < 3 ? 1.f : 2.f) * sig[e] * sig[e];
+        }
+        const float dpw = pm ? pm->dp_weight : 0.f;
+        if constexpr (MODE == 0) {
+            const float U[3] = {u[0] * a.vel, u[1] * a.vel, u[2] * a.vel};
+            const double R = (double)M.rho * a.dens;
+            const double usq = (double)U[0] * U[0] + (double)U[1] * U[1] + (double)U[2] * U[2];
+            acc.add(0, U[0]);
+            acc.add(1, U[1]);
+            acc.add(2, U[2]);
+            acc.add(3, R * usq);
+            acc.add(4, R * alpha / a.dt_s * usq);
+            acc.add(5, (double)a.phi[x]);
+            if (pm) acc.add(6, (double)dpw * a.dens * (double)M.rp * a.vel * a.vel / 3.0);
+            acc.add(7, (double)ss / (2.0 * M.rho * nu));
+            if (a.fields) {
+                a.fields[x] = M.rp;
+                a.fields[n + x] = u[0];
+                a.fields[2 * n + x] = u[1];
+                a.fields[3 * n + x] = u[2];
+            }
+        } else {
+            // cotangents of rho, u, F, M2 (all lattice units)
+            const float V = a.vel;
+            const float U[3] = {u[0] * V, u[1] * V, u[2] * V};
+            const float usq = U[0] * U[0] + U[1] * U[1] + U[2] * U[2];
+            const float R = M.rho * a.dens;
+            const float W3 = (float)a.w[3], W4 = (float)a.w[4], W7 = (float)a.w[7];
+            float rb = 0.f, abar = 0.f, ub[3], Fb[3] = {0.f, 0.f, 0.f}, Sb[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            const float kin = W3 + W4 * alpha / a.dt_s;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) ub[d] = (float)a.w[d] * V + kin * R * 2.f * U[d] * V;
+            rb += kin * a.dens * usq;
+            abar += W4 * R / a.dt_s * usq;
+            if (pm) rb += (float)a.w[6] * dpw * a.dens * V * V / 3.f;
+            if (W7 != 0.f) {
+                rb += -W7 * ss / (2.f * M.rho * M.rho * nu);
+#pragma unroll
+                for (int e = 0; e < 6; ++e) {
+                    const float mult = (e < 3 ? 1.f : 2.f);  // off-diagonals appear twice
+                    const float pb = -k * W7 * sig[e] / (M.rho * nu) * mult;
+                    const int i0 = ia[e], i1 = ib[e];
+                    Sb[e] += pb;
+                    rb -= pb * ((e < 3 ? 1.f / 3.f : 0.f) + u[i0] * u[i1]);
+                    if (e < 3) {
+                        ub[i0] -= 2.f * M.rho * pb * u[i0];
+                        ub[i0] += pb * F[i0];
+                        Fb[i0] += pb * u[i0];
+                    } else {
+                        ub[i0] -= M.rho * pb * u[i1];
+                        ub[i1] -= M.rho * pb * u[i0];
+                        ub[i0] += 0.5f * pb * F[i1];
+                        ub[i1] += 0.5f * pb * F[i0];
+                        Fb[i1] += 0.5f * pb * u[i0];
+                        Fb[i0] += 0.5f * pb * u[i1];
+                    }
+                }
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                rb += Fb[d] * (a.P.a[d] - alpha * u[d]);
+                abar -= Fb[d] * M.rho * u[d];
+                ub[d] -= Fb[d] * M.rho * alpha;
+            }
+            const float s = 1.f + 0.5f * alpha;
+            const float inv = 1.f / (s * M.rho);
+            float mb[3], sbar = 0.f;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                mb[d] = ub[d] * inv;
+                rb -= ub[d] * (s * u[d] - 0.5f * a.P.a[d]) * inv;
+                sbar -= ub[d] * u[d] / s;
+            }
+            abar += 0.5f * sbar;
+            float fb[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const int c0 = L::cx(q), c1 = L::cy(q), c2 = L::cz(q);
+                float v = rb;
+                if (c0) v += c0 * mb[0] + Sb[0];
+                if (c1) v += c1 * mb[1] + Sb[1];
+                if (c2) v += c2 * mb[2] + Sb[2];
+                if (c0 && c1) v += c0 * c1 * Sb[3];
+                if (c0 && c2) v += c0 * c2 * Sb[4];
+                if (c1 && c2) v += c1 * c2 * Sb[5];
+                fb[q] = v;
+            }
+            a.abar_final[x] = abar;
+            a.phibar[x] = (float)a.w[5];
+            if (a.record) {
+                a.record[x] = M.rp;
+                a.record[n + x] = u[0];
+                a.record[2 * n + x] = u[1];
+                a.record[3 * n + x] = u[2];
+            }
+            if (a.port_transpose && pm) port_transpose<Q>(*pm, fb);
+            if (a.write_lambda) {
+                TL* B = static_cast<TL*>(a.lam);
+#pragma unroll
+                for (int q = 0; q < Q; ++q) B[opp<Q>(q) * n + x] = Cvt<TL>::from(fb[q] * a.lam_scale);
+            }
+            if (a.norm2) {
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    const float sv = fb[q] * a.lam_scale;
+                    nsum += (double)sv * (double)sv;
+                }
+            }
+        }
+    }
+    if constexpr (MODE == 0) {
+        finish_sums<8>(acc, a.sums, a.red);
+    } else {
+        if (a.norm2) {
+            Sums<1> s;
+            s.init();
+            s.h[0] = nsum;
+            finish_sums<1>(s, a.norm2, a.red);
+        }
+    }
+}
+
+template <int Q, typename T>
+__global__ void __launch_bounds__(BLOCK) k_canon_pop(Geometry G, const T* A, const uint32_t* __restrict__ mask,
+                                                     const PortMap* ports, int parity, int apply_ports, float* out) {
+    for (uint32_t x = blockIdx.x * BLOCK + threadIdx.x; x < (uint32_t)G.n; x += gridDim.x * BLOCK) {
+        const uint32_t m = mask[x];
+        float g[Q];
+        if (m & MASK_SOLID) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) g[q] = pdec<Q, T>(A[(int64_t)q * G.n + x], q);
+        } else {
+            load_pop<Q, T>(A, G, x, m, parity, g);
+            if (apply_ports && (m & MASK_PORT)) apply_port<Q>(ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], g);
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) out[(int64_t)q * G.n + x] = g[q];
+    }
+}
+
+template <int Q, typename T>
+__global__ void __launch_bounds__(BLOCK) k_upload_pop(Geometry G, T* A, const float* in) {
+    for (int64_t x = (int64_t)blockIdx.x * BLOCK + threadIdx.x; x < G.n; x += (int64_t)gridDim.x * BLOCK) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) A[(int64_t)q * G.n + x] = penc<Q, T>(in[(int64_t)q * G.n + x], q);
+    }
+}
+
+// Natural-order lambda after an adjoint step (after_odd) or after a seed /
+// parity-0 adjoint step.
+template <int Q, typename T>
+__global__ void __launch_bounds__(BLOCK) k_canon_lam(Geometry G, const T* B, const uint32_t* __restrict__ mask,
+                                                     int after_odd, float inv_scale, float* out) {
+    using L = Lat<Q>;
+    for (int64_t x = (int64_t)blockIdx.x * BLOCK + threadIdx.x; x < G.n; x += (int64_t)gridDim.x * BLOCK) {
+        const uint32_t m = mask[x];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            float v = 0.f;
+            if (!(m & MASK_SOLID)) {
+                const uint32_t n = (uint32_t)G.n;
+                uint32_t idx;
+                if (!after_odd || (m & (1u << q))) idx = opp<Q>(q) * n + (uint32_t)x;
+                else idx = q * n + neighbor(G, (uint32_t)x, m, -L::cx(q), -L::cy(q), -L::cz(q));
+                v = Cvt<T>::to(B[idx]) * inv_scale;
+            }
+            out[(int64_t)q * G.n + x] = v;
+        }
+    }
+}
+
+// Natural lambda (cotangent of the post-port state) -> stored seed layout.
+template <int Q, typename T>
+__global__ void __launch_bounds__(BLOCK) k_seed_lam(Geometry G, T* B, const uint32_t* __restrict__ mask,
+                                                    const PortMap* ports, const float* in, float scale,
+                                                    int port_transpose_on) {
+    for (int64_t x = (int64_t)blockIdx.x * BLOCK + threadIdx.x; x < G.n; x += (int64_t)gridDim.x * BLOCK) {
+        const uint32_t m = mask[x];
+        if (m & MASK_SOLID) continue;
+        float v[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) v[q] = in[(int64_t)q * G.n + x];
+        if (port_transpose_on && (m & MASK_PORT)) port_transpose<Q>(ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], v);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) B[opp<Q>(q) * G.n + x] = Cvt<T>::from(v[q] * scale);
+    }
+}
+
+// ------------------------------------------------------------------ design
+__device__ __forceinline__ bool shifted(const Geometry& G, int64_t x, int dx, int dy, int dz, int64_t& out) {
+    int64_t i, j, k;
+    coords(G, x, i, j, k);
+    i += dx;
+    j += dy;
+    k += dz;
+    if (i < 0 || i >= G.nx) {
+        if (!(G.periodic & 1)) return false;
+        i = (i % G.nx + G.nx) % G.nx;
+    }
+    if (j < 0 || j >= G.ny) {
+        if (!(G.periodic & 2)) return false;
+        j = (j % G.ny + G.ny) % G.ny;
+    }
+    if (k < 0 || k >= G.nz) {
+        if (!(G.periodic & 4)) return false;
+        k = (k % G.nz + G.nz) % G.nz;
+    }
+    out = (i * G.ny + j) * G.nz + k;
+    return true;
+}
+
+// DesignMap::map + resistance (design.rs:199-216, 284-286).
+__global__ void __launch_bounds__(BLOCK) k_design_map(DesignArgs a) {
+    for (int64_t x = (int64_t)blockIdx.x * BLOCK + threadIdx.x; x < a.G.n; x += (int64_t)gridDim.x * BLOCK) {
+        const uint8_t c = a.cls[x];
+        float phi, den = 1.f, slope = 0.f;
+        if (c == 0) phi = 0.f;
+        else if (c == 2) phi = a.fixed[x];
+        else {
+            float f;
+            if (a.n_offsets == 0) f = a.raw[x];
+            else {
+                float num = 0.f, dsum = 0.f;
+                for (int o = 0; o < a.n_offsets; ++o) {
+                    const int4 off = a.offsets[o];
+                    int64_t src;
+                    if (!shifted(a.G, x, -off.x, -off.y, -off.z, src)) continue;
+                    if (a.cls[src] != 1) continue;
+                    const float wgt = __int_as_float(off.w);
+                    num = fmaf(wgt, a.raw[src], num);
+                    dsum += wgt;
+                }
+                den = dsum > 0.f ? dsum : 1.f;
+                f = num / den;
+            }
+            if (a.beta > 0.f) {
+                const float t = tanhf(a.beta * (f - a.eta));
+                phi = (a.proj_a + t) / a.proj_den;
+                slope = a.beta * (1.f - t * t) / a.proj_den;
+            } else {
+                phi = f;
+                slope = 1.f;
+            }
+        }
+        a.phi[x] = phi;
+        a.alpha[x] = a.ramp_c * (1.f - phi) / (a.ramp_q + phi);
+        a.den[x] = den;
+        a.slope[x] = slope;
+    }
+}
+
+// phi_bar += (abar + abar_final) d alpha / d phi; then the projection slope
+// and the filter normalisation (provider.rs:352-354, design.rs:219-243).
+__global__ void __launch_bounds__(BLOCK) k_sens_scale(DesignArgs a) {
+    for (int64_t x = (int64_t)blockIdx.x * BLOCK + threadIdx.x; x < a.G.n; x += (int64_t)gridDim.x * BLOCK) {
+        float v = 0.f;
+        if (a.cls[x] == 1) {
+            const float phi = a.phi[x];
+            const float d = a.ramp_q + phi;
+            const float dres = a.ramp_c * (-d - (1.f - phi)) / (d * d);
+            float ab = 0.f;
+            if (a.abar) ab += a.abar[x] * a.abar_scale;
+            if (a.abar_final) ab += a.abar_final[x];
+            const float pb = a.phibar[x] + ab * dres;
+            v = pb * a.slope[x] / a.den[x];
+        }
+        a.scale[x] = v;
+    }
+}
+
+__global__ void __launch_bounds__(BLOCK) k_filter_transpose(DesignArgs a) {
+    for (int64_t s = (int64_t)blockIdx.x * BLOCK + threadIdx.x; s < a.G.n; s += (int64_t)gridDim.x * BLOCK) {
+        float g = 0.f;
+        if (a.cls[s] == 1) {
+            if (a.n_offsets == 0) g = a.scale[s];
+            else {
+                for (int o = 0; o < a.n_offsets; ++o) {
+                    const int4 off = a.offsets[o];
+                    int64_t x;
+                    if (!shifted(a.G, s, off.x, off.y, off.z, x)) continue;
+                    g = fmaf(__int_as_float(off.w), a.scale[x], g);
+                }
+            }
+        }
+        a.grad[s] = g;
+    }
+}
+
+
+}  // namespace
+
+cudaError_t launch_init(int Q, int storage, const Geometry& G, const Physics& P, void* pop, const uint32_t* mask,
+                        cudaStream_t s) {
+    const int grid = blocks_for(G.n, 0);
+    if (Q == 19) {
+        LBM_STORAGE_DISPATCH(storage, T, k_init<19, T><<<grid, BLOCK, 0, s>>>(G, P, static_cast<T*>(pop), mask))
+    } else {
+        LBM_STORAGE_DISPATCH(storage, T, k_init<27, T><<<grid, BLOCK, 0, s>>>(G, P, static_cast<T*>(pop), mask))
+    }
+    return cudaGetLastError();
+}
+
+template <int Q, typename T>
+static void objective_dispatch(int lstorage, int mode, const ObjArgs& a, int grid, cudaStream_t s) {
+    if (mode == 0) {
+        k_objective<Q, T, float, 0><<<persistent_grid((const void*)k_objective<Q, T, float, 0>, a.G.n), BLOCK, 0, s>>>(a);
+    } else {
+        LBM_STORAGE_DISPATCH(lstorage, TL, k_objective<Q, T, TL, 1><<<persistent_grid((const void*)k_objective<Q, T, TL, 1>, a.G.n), BLOCK, 0, s>>>(a))
+    }
+}
+
+cudaError_t launch_objective(int Q, int storage, int lstorage, int mode, const ObjArgs& a, int grid,
+                             cudaStream_t s) {
+    if (Q == 19) {
+        LBM_STORAGE_DISPATCH(storage, T, objective_dispatch<19, T>(lstorage, mode, a, grid, s))
+    } else {
+        LBM_STORAGE_DISPATCH(storage, T, objective_dispatch<27, T>(lstorage, mode, a, grid, s))
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_canon_pop(int Q, int storage, const Geometry& G, const void* pop, const uint32_t* mask,
+                             const PortMap* ports, int parity, int apply_ports, float* out, int grid,
+                             cudaStream_t s) {
+    if (Q == 19) {
+        LBM_STORAGE_DISPATCH(storage, T,
+                             k_canon_pop<19, T><<<grid, BLOCK, 0, s>>>(G, static_cast<const T*>(pop), mask, ports,
+                                                                        parity, apply_ports, out))
+    } else {
+        LBM_STORAGE_DISPATCH(storage, T,
+                             k_canon_pop<27, T><<<grid, BLOCK, 0, s>>>(G, static_cast<const T*>(pop), mask, ports,
+                                                                        parity, apply_ports, out))
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_upload_pop(int Q, int storage, const Geometry& G, void* pop, const float* in, int grid,
+                              cudaStream_t s) {
+    if (Q == 19) {
+        LBM_STORAGE_DISPATCH(storage, T, k_upload_pop<19, T><<<grid, BLOCK, 0, s>>>(G, static_cast<T*>(pop), in))
+    } else {
+        LBM_STORAGE_DISPATCH(storage, T, k_upload_pop<27, T><<<grid, BLOCK, 0, s>>>(G, static_cast<T*>(pop), in))
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_canon_lam(int Q, int lstorage, const Geometry& G, const void* lam, const uint32_t* mask,
+                             int after_odd, float inv_scale, float* out, int grid, cudaStream_t s) {
+    if (Q == 19) {
+        LBM_STORAGE_DISPATCH(lstorage, T,
+                             k_canon_lam<19, T><<<grid, BLOCK, 0, s>>>(G, static_cast<const T*>(lam), mask,
+                                                                        after_odd, inv_scale, out))
+    } else {
+        LBM_STORAGE_DISPATCH(lstorage, T,
+                             k_canon_lam<27, T><<<grid, BLOCK, 0, s>>>(G, static_cast<const T*>(lam), mask,
+                                                                        after_odd, inv_scale, out))
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_seed_lam(int Q, int lstorage, const Geometry& G, void* lam, const uint32_t* mask,
+                            const PortMap* ports, const float* in, float scale, int port_transpose_on, int grid,
+                            cudaStream_t s) {
+    if (Q == 19) {
+        LBM_STORAGE_DISPATCH(lstorage, T,
+                             k_seed_lam<19, T><<<grid, BLOCK, 0, s>>>(G, static_cast<T*>(lam), mask, ports, in,
+                                                                       scale, port_transpose_on))
+    } else {
+        LBM_STORAGE_DISPATCH(lstorage, T,
+                             k_seed_lam<27, T><<<grid, BLOCK, 0, s>>>(G, static_cast<T*>(lam), mask, ports, in,
+                                                                       scale, port_transpose_on))
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_design_map(const DesignArgs& a, int grid, cudaStream_t s) {
+    k_design_map<<<grid, BLOCK, 0, s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_sens_scale(const DesignArgs& a, int grid, cudaStream_t s) {
+    k_sens_scale<<<grid, BLOCK, 0, s>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_filter_transpose(const DesignArgs& a, int grid, cudaStream_t s) {
+    k_filter_transpose<<<grid, BLOCK, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+
+
+}  // namespace lbm

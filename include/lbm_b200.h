@@ -160,7 +160,10 @@ typedef struct {
 } lbm_problem_t;
 
 /* Trajectory admission record (solver.rs:708-793).  Filled by lbm_forward
- * and lbm_advance. */
+ * and lbm_advance.  A trajectory is admitted when every population of every
+ * state is finite and positive, the Mach number stays within mach_limit and
+ * the relative mass drift is at most 1e-6 (FP32 storage, the reference's
+ * bound), 1e-4 (FP16) or 1e-3 (BF16 storage). */
 typedef struct {
     double maximum_mach;          /* sqrt(3) * max |u| over fluid cells and states */
     double relative_mass_drift;   /* max_t |M_t - (M_0 + sum exchange)| / M_0 */
@@ -257,6 +260,15 @@ LBM_API lbm_status lbm_forward(lbm_handle* h, int64_t steps, lbm_diag_t* diag);
 LBM_API lbm_status lbm_set_populations(lbm_handle* h, const double* f, size_t n);
 LBM_API lbm_status lbm_get_populations(lbm_handle* h, double* f, size_t n);
 LBM_API lbm_status lbm_advance(lbm_handle* h, int64_t steps, lbm_diag_t* diag);
+
+/* Per-state admission record of the last lbm_forward / lbm_advance
+ * (admit, solver.rs:708-793): for states t = 0..steps, the fluid mass
+ * sum(rho), the port mass exchange of the step that produced the state
+ * (0 for t = 0; the reference's boundary_mass_changes_lattice), the minimum
+ * population and the maximum speed |u| over fluid cells.  n = steps + 1;
+ * any pointer may be NULL. */
+LBM_API lbm_status lbm_trajectory(lbm_handle* h, double* mass, double* exchange, double* min_population,
+                                  double* max_speed, size_t n);
 
 /* The 8 responses of the current state (LBM_R_*), FP64 compensated sums. */
 LBM_API lbm_status lbm_responses(lbm_handle* h, double* out8);

@@ -1213,8 +1213,16 @@ double orc_interval(const orc_problem* o, const double* before, const double* al
     return interval(*o, before, alpha, after, post);
 }
 
+void orc_history_trace(const orc_problem* o, const double* alpha, int64_t steps, double* final_state,
+                       orc_diag_t* diag, double* mass_out, double* exch_out);
+
 void orc_history(const orc_problem* o, const double* alpha, int64_t steps, double* final_state,
                  orc_diag_t* diag) {
+    orc_history_trace(o, alpha, steps, final_state, diag, nullptr, nullptr);
+}
+
+void orc_history_trace(const orc_problem* o, const double* alpha, int64_t steps, double* final_state,
+                       orc_diag_t* diag, double* mass_out, double* exch_out) {
     const int64_t NQ = o->N * o->Q;
     std::vector<double> a(NQ), b(NQ), post;
     initial(*o, a.data());
@@ -1251,6 +1259,10 @@ void orc_history(const orc_problem* o, const double* alpha, int64_t steps, doubl
         diag->admitted = (finite && minimum > 0 && mach <= o->mach_limit && err <= 1e-6) ? 1 : 0;
     }
     if (final_state) std::memcpy(final_state, a.data(), sizeof(double) * NQ);
+    for (int64_t t = 0; t <= steps; ++t) {
+        if (mass_out) mass_out[t] = mass[t];
+        if (exch_out) exch_out[t] = t == 0 ? 0.0 : changes[t - 1];
+    }
 }
 
 void orc_vector(const orc_problem* o, const double* phi, const double* alpha, const double* f, double* out8) {

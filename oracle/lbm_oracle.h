@@ -64,6 +64,11 @@ double orc_interval(const orc_problem* o, const double* before, const double* al
 void orc_history(const orc_problem* o, const double* alpha, int64_t steps, double* final_state,
                  orc_diag_t* diag);
 
+/* orc_history plus the per-state fluid mass [steps+1] and the exchange of
+ * the step producing each state [steps+1] (entry 0 is zero). */
+void orc_history_trace(const orc_problem* o, const double* alpha, int64_t steps, double* final_state,
+                       orc_diag_t* diag, double* mass, double* exchange);
+
 /* vector responses (solver.rs:874-893 plus pressure drop and viscous
  * dissipation) and their VJP (solver.rs:896-947) */
 void orc_vector(const orc_problem* o, const double* phi, const double* alpha, const double* f, double* out8);

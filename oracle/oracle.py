@@ -71,6 +71,8 @@ def lib() -> C.CDLL:
         L.orc_interval.restype = C.c_double
         L.orc_history.argtypes = [h, _dp, C.c_int64, _dp, C.POINTER(Diag)]
         L.orc_history.restype = None
+        L.orc_history_trace.argtypes = [h, _dp, C.c_int64, _dp, C.POINTER(Diag), _dp, _dp]
+        L.orc_history_trace.restype = None
         L.orc_vector.argtypes = [h, _dp, _dp, _dp, _dp]
         L.orc_vector.restype = None
         L.orc_vector_vjp.argtypes = [h, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
@@ -166,6 +168,14 @@ class Oracle:
         d = Diag()
         lib().orc_history(self.h, _p(al), int(steps), _p(f), C.byref(d))
         return f.reshape(self.cells, self.q), d
+
+    def history_trace(self, alpha, steps):
+        al = np.ascontiguousarray(alpha, dtype=np.float64)
+        f = np.empty(self.cells * self.q)
+        mass, exch = np.empty(steps + 1), np.empty(steps + 1)
+        d = Diag()
+        lib().orc_history_trace(self.h, _p(al), int(steps), _p(f), C.byref(d), _p(mass), _p(exch))
+        return f.reshape(self.cells, self.q), d, mass, exch
 
     def vector(self, phi, alpha, f):
         out = np.empty(8)

@@ -147,7 +147,8 @@ def test_horizon_gradient_matches_oracle(gpu_lib, coll, lattice, response):
     with LbmSolver(prob) as s:
         s.set_design(raw)
         g, rep = s.gradient(w, mode="horizon", checkpoint_every=13)
-    assert rep.iterations == 60
+    # the fluid volume does not depend on the populations: no adjoint steps needed
+    assert rep.iterations == (0 if response == 5 else 60)
     assert rel_l2(g, g_ref) < 1e-4, rel_l2(g, g_ref)
 
 
