@@ -23,7 +23,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import subprocess
 import sys
@@ -131,36 +130,17 @@ class Clocks:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup(n_gpus):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        from datetime import timedelta
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-    return rank, world, local
-
-
 def barrier_max(value, world):
-    if world <= 1:
-        return value
-    import torch
-    import torch.distributed as dist
+    from implexity_b200 import replicas
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return replicas.max_over_ranks(value) if world > 1 else value
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
+    from implexity_b200 import replicas
 
-        dist.barrier()
+    if world > 1:
+        replicas.barrier()
 
 
 def run_gpu(args, rank, world, local):
@@ -362,15 +342,14 @@ def main():
         }
         print(json.dumps(line))
         return
-    rank, world, local = dist_setup(args.gpus)
+    from implexity_b200 import replicas
+
+    rank, world, local = replicas.init("nccl")
     res = run_gpu(args, rank, world, local)
     cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_sample(args.config, seconds_target=args.cpu_seconds)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
+    replicas.finalize()
     if rank != 0:
         return
     head = res.get("fp32") or next(iter(res.values()))
