@@ -42,6 +42,7 @@ EXPORTS = [
     "lbm_gradient",
     "lbm_step_vjp",
     "lbm_design_vjp",
+    "lbm_state_stats_noalloc",
 ]
 
 
@@ -164,6 +165,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.lbm_gradient.argtypes = [h, _dp, C.POINTER(AdjointOpts), _dp, C.POINTER(AdjointReport)]
     lib.lbm_step_vjp.argtypes = [h, _dp, _dp, _dp, _dp, C.c_size_t]
     lib.lbm_design_vjp.argtypes = [h, _dp, _dp, C.c_size_t]
+    lib.lbm_state_stats_noalloc.argtypes = [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, _dp,
+                                            C.c_void_p, C.c_void_p]
     for name in EXPORTS:
         fn = getattr(lib, name)
         if name not in ("lbm_destroy", "lbm_last_error"):

@@ -120,6 +120,10 @@ struct DesignArgs {
 // (parity 1), aligned down to `vec` elements.
 void run_table(int Q, const Geometry& G, int parity, int dir, int vec, int64_t* run0, int32_t* rund);
 
+// Sets the message lbm_last_error(NULL) returns on this thread (entry points
+// that take no handle report through it).
+void set_thread_error(const char* msg);
+
 cudaError_t launch_init(int Q, int storage, const Geometry& G, const Physics& P, void* pop, const uint32_t* mask,
                         cudaStream_t s);
 cudaError_t launch_forward(int Q, int coll, int storage, const FwdArgs& a, int grid, cudaStream_t s);

@@ -1200,6 +1200,10 @@ void check_n(const lbm_handle& h, size_t n, size_t expect, const char* what) {
 
 }  // namespace
 
+namespace lbm {
+void set_thread_error(const char* msg) { g_create_error = msg; }
+}  // namespace lbm
+
 // ================================================================ C ABI
 extern "C" {
 

@@ -298,6 +298,40 @@ LBM_API lbm_status lbm_step_vjp(lbm_handle* h, const double* state, const double
  * design last set: out[N] = d phi / d raw ^T phi_bar. */
 LBM_API lbm_status lbm_design_vjp(lbm_handle* h, const double* phi_bar, double* out, size_t n);
 
+/* ---- state statistics without device allocation ------------------------ */
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- code inside another framework's memory pool or arena (the pool
+ * owns all device memory), code that runs while a CUDA graph is being
+ * captured, embedded hosts that fix their device budget up front -- and that
+ * already hold a state on the device: the admission statistics of that one
+ * state, computed by the same compensated reduction the stepping kernels run
+ * every step (LbmProblem::admit quantities, solver.rs:714-755).
+ *
+ *   populations  device, FP32, plane-major f[q*cells + cell] (unshifted f),
+ *                velocity order of the lattice as in lbm_get_populations
+ *   solid        device uint8 per cell, NULL = all fluid (solid cells skipped)
+ *   alpha        device FP32 Brinkman resistance per cell, NULL = 0
+ *   acceleration_lattice  host, 3 doubles, NULL = 0
+ *   out4         device, 4 doubles: fluid mass sum(rho), minimum population,
+ *                maximum |u| (implicit half-step Brinkman velocity), and 1.0
+ *                if any population is non-finite (else 0.0)
+ *   stream       cudaStream_t, NULL = the legacy default stream
+ *
+ * It allocates nothing: its scratch (per-block partials and a ticket counter)
+ * is a 65 792-byte static device array that every GPU loading the library
+ * holds until the process exits.  Limit: q * cells < 2^31 (larger states are
+ * rejected with LBM_E_CONTRACT); any such state is covered with at most 1024
+ * blocks.  The first call on a device looks up the array's device address on
+ * that device, so make that first call before any stream capture.  The call is
+ * asynchronous on `stream`: out4 is written when the stream reaches the
+ * kernel.  All calls share the one array, so calls that overlap on the GPU
+ * (other streams, other host threads, same device) race and must be ordered
+ * by the caller.  Errors are reported through lbm_last_error(NULL). */
+LBM_API lbm_status lbm_state_stats_noalloc(int32_t q, int64_t cells, const float* populations,
+                                           const uint8_t* solid, const float* alpha,
+                                           const double* acceleration_lattice, double* out4, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
