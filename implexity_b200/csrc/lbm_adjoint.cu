@@ -1,13 +1,15 @@
 // lbm_adjoint.cu -- one transposed step of the discrete adjoint.
 //
-// interval_vjp (solver.rs:642-674) restated for the AA layout: the adjoint
-// populations stream with the velocities reversed (the transpose of the pull
-// of Streaming::stream, solver.rs:131-157), the collision transpose is taken
-// at the recorded forward (rho, u) (collide_pairs_vjp, moving/collision.rs:
-// 492-570, with the Brinkman chain of moving/psm.rs:402-486), the alpha
-// cotangent accumulates per cell, and port cells apply the transposed port
-// map (apply_ports_vjp, ports.rs:582-621) before storing.  Loads are staged
-// like the forward step (lbm_device.cuh).
+// interval_vjp (solver.rs:642-674) restated for the two-array layout: the
+// stored adjoint array holds Ports^T C^T of the cotangent of the streamed
+// state; one transposed step pulls it with the velocities reversed (the
+// transpose of the pull of Streaming::stream, solver.rs:131-157), takes the
+// collision transpose at the recorded forward (rho, u) (collide_pairs_vjp,
+// moving/collision.rs:492-570, with the Brinkman chain of moving/psm.rs:
+// 402-486), accumulates the alpha cotangent per cell, applies the transposed
+// port map at port cells (apply_ports_vjp, ports.rs:582-621) and stores into
+// the cell's own slots of the other array.  Loads are staged like the
+// forward step (lbm_device.cuh).
 #include "lbm_device.cuh"
 
 namespace lbm {
@@ -21,13 +23,14 @@ struct AdjStage {
     float alpha[FRUN];
 };
 
-template <int Q, int COLL, typename T, int PAR>
+template <int Q, int COLL, typename T>
 __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
     using S = AdjStage<Q, T>;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
     uint64_t* empty = full + STAGES;
-    T* B = static_cast<T*>(a.lam);
+    const T* B = static_cast<const T*>(a.src);
+    T* D = static_cast<T*>(a.dst);
     const uint32_t n = (uint32_t)a.G.n;
     const uint32_t ntiles = (n + TILE - 1) / TILE;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -63,41 +66,49 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
             }
         }
     } else {
-        const int c = threadIdx.x - 32;
+        const int c0 = threadIdx.x - 32;
         int s = 0;
         uint32_t round = 0;
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
             const bool ok = mbar_wait(&full[s], round & 1u, a.err);
             const S* st = stage_at<S>(smem, s);
-            const uint32_t x = tile * TILE + c;
-            if (ok && x < n) {
-                const uint32_t m = st->mask[c];
-                if (!(m & MASK_SOLID)) {
-                    float v[Q];
-                    if (PAR == 0 || !(m & MASK_WRAP)) {
+#pragma unroll 1
+            for (int k = 0; k < CPT; ++k) {
+                const int c = c0 + k * (CONSUMER_WARPS * 32);
+                const uint32_t x = tile * TILE + c;
+                if (ok && x < n) {
+                    const uint32_t m = st->mask[c];
+                    if (!(m & MASK_SOLID)) {
+                        float v[Q];
+                        if (!(m & MASK_WRAP)) {
 #pragma unroll
-                        for (int q = 0; q < Q; ++q) {
-                            T r;
-                            if (PAR == 1 && ((m >> opp<Q>(q)) & 1u)) r = B[q * n + x];
-                            else r = st->run[q][a.rund[q] + c];
-                            v[q] = Cvt<T>::to(r) * a.in_scale_inv;
+                            for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(st->run[q][a.rund[q] + c]);
+                            if (m & LINK_BITS) {
+                                // transposed bounce-back: the cell's own opposite slot
+#pragma unroll
+                                for (int q = 1; q < Q; ++q)
+                                    if ((m >> opp<Q>(q)) & 1u) v[q] = Cvt<T>::to(B[opp<Q>(q) * n + x]);
+                            }
+#pragma unroll
+                            for (int q = 0; q < Q; ++q) v[q] *= a.in_scale_inv;
+                        } else {
+#pragma unroll
+                            for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(B[pull_adj_index<Q>(a.G, x, m, q)]) * a.in_scale_inv;
                         }
-                    } else {
-                        load_lam<Q, T>(B, a.G, x, m, PAR, a.in_scale_inv, v);
-                    }
-                    const float u[3] = {st->rec[1][a.recd[1] + c], st->rec[2][a.recd[2] + c],
-                                        st->rec[3][a.recd[3] + c]};
-                    const float ab = collide_vjp<Q, COLL>(v, st->rec[0][a.recd[0] + c], u, st->alpha[c], a.P);
-                    if (a.overwrite_abar) a.abar[x] = ab * a.abar_factor;
-                    else a.abar[x] = fmaf(ab, a.abar_factor, a.abar[x]);
-                    if (a.port_transpose && (m & MASK_PORT))
-                        port_transpose<Q>(a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], v);
-                    store_lam_p<Q, T, PAR>(B, a.G, x, m, a.out_scale, v);
-                    if (a.norm2) {
+                        const float u[3] = {st->rec[1][a.recd[1] + c], st->rec[2][a.recd[2] + c],
+                                            st->rec[3][a.recd[3] + c]};
+                        const float ab = collide_vjp<Q, COLL>(v, st->rec[0][a.recd[0] + c], u, st->alpha[c], a.P);
+                        if (a.overwrite_abar) a.abar[x] = ab * a.abar_factor;
+                        else a.abar[x] = fmaf(ab, a.abar_factor, a.abar[x]);
+                        if (a.port_transpose && (m & MASK_PORT))
+                            port_transpose<Q>(a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], v);
+                        store_own_lam<Q, T>(D, n, x, v, a.out_scale);
+                        if (a.norm2) {
 #pragma unroll
-                        for (int q = 0; q < Q; ++q) {
-                            const float sv = v[q] * a.out_scale;
-                            nsum += (double)sv * (double)sv;
+                            for (int q = 0; q < Q; ++q) {
+                                const float sv = v[q] * a.out_scale;
+                                nsum += (double)sv * (double)sv;
+                            }
                         }
                     }
                 }
@@ -118,23 +129,18 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
     }
 }
 
-template <int Q, int COLL, typename T, int PAR>
+template <int Q, int COLL, typename T>
 cudaError_t run_adjoint(const AdjArgs& a, cudaStream_t s) {
     constexpr size_t smem = pipe_bytes<AdjStage<Q, T>>();
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = set_smem(k_adjoint<Q, COLL, T, PAR>, smem);
+        cudaError_t e = set_smem(k_adjoint<Q, COLL, T>, smem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    const int grid = persistent_grid((const void*)k_adjoint<Q, COLL, T, PAR>, a.G.n, smem, TPB, TILE);
-    k_adjoint<Q, COLL, T, PAR><<<grid, TPB, smem, s>>>(a);
+    const int grid = persistent_grid((const void*)k_adjoint<Q, COLL, T>, a.G.n, smem, TPB, TILE);
+    k_adjoint<Q, COLL, T><<<grid, TPB, smem, s>>>(a);
     return cudaGetLastError();
-}
-
-template <int Q, int COLL, typename T>
-cudaError_t run_adjoint_p(const AdjArgs& a, cudaStream_t s) {
-    return a.parity == 0 ? run_adjoint<Q, COLL, T, 0>(a, s) : run_adjoint<Q, COLL, T, 1>(a, s);
 }
 
 }  // namespace
@@ -142,7 +148,7 @@ cudaError_t run_adjoint_p(const AdjArgs& a, cudaStream_t s) {
 cudaError_t launch_adjoint(int Q, int coll, int lstorage, const AdjArgs& a0, int grid, cudaStream_t s) {
     (void)grid;
     AdjArgs a = a0;
-    run_table(Q, a.G, a.parity, +1, lstorage == ST_F32 ? 4 : 8, a.run0, a.rund);
+    run_table(Q, a.G, +1, lstorage == ST_F32 ? 4 : 8, a.run0, a.rund);
     for (int k = 0; k < 4; ++k) {
         const int64_t first = (int64_t)k * a.G.n;
         a.recd[k] = (int32_t)(first % 4);
@@ -150,15 +156,15 @@ cudaError_t launch_adjoint(int Q, int coll, int lstorage, const AdjArgs& a0, int
     }
     if (Q == 19) {
         if (coll == CK_MRT) {
-            LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint_p<19, CK_MRT, T>(a, s))
+            LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint<19, CK_MRT, T>(a, s))
         } else {
-            LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint_p<19, CK_PAIRS, T>(a, s))
+            LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint<19, CK_PAIRS, T>(a, s))
         }
     } else {
         if (coll == CK_MRT) {
-            LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint_p<27, CK_MRT, T>(a, s))
+            LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint<27, CK_MRT, T>(a, s))
         } else {
-            LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint_p<27, CK_PAIRS, T>(a, s))
+            LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint<27, CK_PAIRS, T>(a, s))
         }
     }
     return cudaGetLastError();

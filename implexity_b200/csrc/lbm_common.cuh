@@ -82,6 +82,7 @@ LBM_HD constexpr int opp(int q) {
 //   bits 28..30  port index + 1 (0: not a port cell)
 //   bit 31       solid cell (inert; never read or written by the stepping)
 constexpr uint32_t MASK_WRAP = 1u << 27;
+constexpr uint32_t LINK_BITS = (1u << 27) - 1u;  // the per-direction blocked-link bits
 constexpr uint32_t MASK_PORT_SHIFT = 28;
 constexpr uint32_t MASK_PORT = 7u << 28;
 constexpr uint32_t MASK_SOLID = 1u << 31;
@@ -117,6 +118,9 @@ struct Physics {
     float proj_rate[MAX_PROJ];     // (s_g - omega) for each corrected moment
     float proj_left[MAX_PROJ][27]; // w_i b_i / |b|^2_W  (reconstruction side)
     float proj_right[MAX_PROJ][27];// b_i                (projection side)
+    float proj_lw[MAX_PROJ][27];   // b_i / |b|^2_W      (reconstruction side, in (f-w)/w units)
+    float proj_m0[MAX_PROJ];       // sum_i w_i b_i
+    float proj_m2[MAX_PROJ][6];    // sum_i w_i b_i c_ia c_ib (xx yy zz xy xz yz)
 };
 
 // Per-step admission reductions (solver.rs:714-755) for one state.

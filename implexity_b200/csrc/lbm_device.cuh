@@ -111,6 +111,19 @@ __device__ __forceinline__ T penc_sr(float g, int q, uint32_t& rs) {
     else return Cvt<T>::from(g);
 }
 
+// Stored element <-> value in storage units: g = f - w for FP32, the
+// weight-relative (f - w)/w for the 16-bit formats (the stepping kernels
+// compute in these units, in which the 16-bit collision needs no weights).
+template <typename T>
+__device__ __forceinline__ float sdec(T v) {
+    return Cvt<T>::to(v);
+}
+template <typename T>
+__device__ __forceinline__ T senc_sr(float v, uint32_t& rs) {
+    if constexpr (Cvt<T>::scaled) return round_stochastic<T>(v, lcg(rs));
+    else return Cvt<T>::from(v);
+}
+
 // ------------------------------------------------------------------ indexing
 // All population indices q*n + x fit in 32 bits (the runtime checks
 // Q*n < 2^32), which keeps the per-direction address arithmetic in 32-bit
@@ -140,148 +153,49 @@ __device__ __forceinline__ void coords(const Geometry& G, int64_t x, int64_t& i,
     i = ij / G.ny;
 }
 
-// Forward AA access.  parity 0 reads own slots; parity 1 gathers the
-// neighbours' opposite slots (own slot when the link is blocked).
-// Linear offset of the neighbour x + c (no wrap): a constant per direction.
+// Linear offset of the neighbour x + sign*c_q (no wrap): a constant per direction.
 template <int Q>
 __device__ __forceinline__ uint32_t lin(const Geometry& G, int q, int sign) {
     using L = Lat<Q>;
     return (uint32_t)(sign * (L::cx(q) * (int)G.sx + L::cy(q) * (int)G.sy + L::cz(q)));
 }
 
-// Forward AA access of the stored elements of one cell.  parity 0 reads the
-// cell's own slots; parity 1 gathers the neighbours' opposite slots (own slot
-// when the link is blocked).  Cells away from periodic faces take the fast
-// path: a select between two addresses per direction, no branches.
-template <int Q, typename T>
-__device__ __forceinline__ void load_raw(const T* __restrict__ A, const Geometry& G, uint32_t x, uint32_t m,
-                                         int parity, T (&r)[Q]) {
+// Two population arrays, each Q planes of n cells.  The current array holds
+// the post-collision populations f*: slot (q, x) = f*_q(x).  One step pulls
+// (Streaming::stream, solver.rs:131-157): f_q(x) = f*_q(x - c_q), or the
+// halfway bounce-back f*_opp(q)(x) when x - c_q is a wall or solid (mask bit
+// q); it collides and writes f*'_q(x) to slot (q, x) of the other array.
+// Every slot of the current array is read by exactly one (cell, direction),
+// so the inverse of the pull (loading a given streamed state) is a scatter
+// through the same index.  Solid cells are never stepped: their own slots
+// hold their populations in both arrays.
+template <int Q>
+__device__ __forceinline__ uint32_t pull_index(const Geometry& G, uint32_t x, uint32_t m, int q) {
     using L = Lat<Q>;
     const uint32_t n = (uint32_t)G.n;
-    if (parity == 0) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) r[q] = A[q * n + x];
-    } else if (!(m & MASK_WRAP)) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const uint32_t own = q * n + x;
-            const uint32_t nb = opp<Q>(q) * n + x + lin<Q>(G, q, -1);
-            r[q] = A[((m >> q) & 1u) ? own : nb];
-        }
-    } else {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            uint32_t idx;
-            if (m & (1u << q)) idx = q * n + x;
-            else idx = opp<Q>(q) * n + neighbor(G, x, m, -L::cx(q), -L::cy(q), -L::cz(q));
-            r[q] = A[idx];
-        }
-    }
+    if (m & (1u << q)) return opp<Q>(q) * n + x;
+    if (!(m & MASK_WRAP)) return q * n + x + lin<Q>(G, q, -1);
+    return q * n + neighbor(G, x, m, -L::cx(q), -L::cy(q), -L::cz(q));
 }
 
-template <int Q, typename T>
-__device__ __forceinline__ void decode(const T (&r)[Q], float (&g)[Q]) {
-#pragma unroll
-    for (int q = 0; q < Q; ++q) g[q] = pdec<Q, T>(r[q], q);
+// Transposed pull of the adjoint step: the cotangent of f*_q(y) gathers from
+// (q, y + c_q), or from the own slot opp(q) when y + c_q is a wall or solid
+// (mask bit opp(q)).
+template <int Q>
+__device__ __forceinline__ uint32_t pull_adj_index(const Geometry& G, uint32_t x, uint32_t m, int q) {
+    using L = Lat<Q>;
+    const uint32_t n = (uint32_t)G.n;
+    if (m & (1u << opp<Q>(q))) return opp<Q>(q) * n + x;
+    if (!(m & MASK_WRAP)) return q * n + x + lin<Q>(G, q, +1);
+    return q * n + neighbor(G, x, m, L::cx(q), L::cy(q), L::cz(q));
 }
 
+// Streamed populations of a fluid cell (g = f - w).
 template <int Q, typename T>
 __device__ __forceinline__ void load_pop(const T* __restrict__ A, const Geometry& G, uint32_t x, uint32_t m,
-                                         int parity, float (&g)[Q]) {
-    T r[Q];
-    load_raw<Q, T>(A, G, x, m, parity, r);
-    decode<Q, T>(r, g);
-}
-
-template <int Q, typename T>
-__device__ __forceinline__ void store_pop(T* A, const Geometry& G, uint32_t x, uint32_t m, int parity,
-                                          const float (&g)[Q], uint32_t step) {
-    using L = Lat<Q>;
-    const uint32_t n = (uint32_t)G.n;
-    uint32_t rs = 0;
-    if constexpr (Cvt<T>::scaled) rs = cell_seed(x, step);
-    if (parity == 0) {
+                                         float (&g)[Q]) {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) A[opp<Q>(q) * n + x] = penc_sr<Q, T>(g[q], q, rs);
-    } else if (!(m & MASK_WRAP)) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            // x + c_q a wall or solid: bounce back into the own opposite slot
-            const uint32_t own = opp<Q>(q) * n + x;
-            const uint32_t nb = q * n + x + lin<Q>(G, q, +1);
-            A[((m >> opp<Q>(q)) & 1u) ? own : nb] = penc_sr<Q, T>(g[q], q, rs);
-        }
-    } else {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            uint32_t idx;
-            if (m & (1u << opp<Q>(q))) idx = opp<Q>(q) * n + x;
-            else idx = q * n + neighbor(G, x, m, L::cx(q), L::cy(q), L::cz(q));
-            A[idx] = penc_sr<Q, T>(g[q], q, rs);
-        }
-    }
-}
-
-// Adjoint AA access (velocities reversed).
-template <int Q, typename T>
-__device__ __forceinline__ void load_lam_raw(const T* __restrict__ B, const Geometry& G, uint32_t x, uint32_t m,
-                                             int parity, T (&r)[Q]) {
-    using L = Lat<Q>;
-    const uint32_t n = (uint32_t)G.n;
-    if (parity == 0) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) r[q] = B[q * n + x];
-    } else if (!(m & MASK_WRAP)) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const uint32_t own = q * n + x;
-            const uint32_t nb = opp<Q>(q) * n + x + lin<Q>(G, q, +1);
-            r[q] = B[((m >> opp<Q>(q)) & 1u) ? own : nb];
-        }
-    } else {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            uint32_t idx;
-            if (m & (1u << opp<Q>(q))) idx = q * n + x;
-            else idx = opp<Q>(q) * n + neighbor(G, x, m, L::cx(q), L::cy(q), L::cz(q));
-            r[q] = B[idx];
-        }
-    }
-}
-
-template <int Q, typename T>
-__device__ __forceinline__ void load_lam(const T* __restrict__ B, const Geometry& G, uint32_t x, uint32_t m,
-                                         int parity, float scale, float (&v)[Q]) {
-    T r[Q];
-    load_lam_raw<Q, T>(B, G, x, m, parity, r);
-#pragma unroll
-    for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(r[q]) * scale;
-}
-
-template <int Q, typename T>
-__device__ __forceinline__ void store_lam(T* B, const Geometry& G, uint32_t x, uint32_t m, int parity, float scale,
-                                          const float (&v)[Q]) {
-    using L = Lat<Q>;
-    const uint32_t n = (uint32_t)G.n;
-    if (parity == 0) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) B[opp<Q>(q) * n + x] = Cvt<T>::from(v[q] * scale);
-    } else if (!(m & MASK_WRAP)) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const uint32_t own = opp<Q>(q) * n + x;
-            const uint32_t nb = q * n + x + lin<Q>(G, q, -1);
-            B[((m >> q) & 1u) ? own : nb] = Cvt<T>::from(v[q] * scale);
-        }
-    } else {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            uint32_t idx;
-            if (m & (1u << q)) idx = opp<Q>(q) * n + x;
-            else idx = q * n + neighbor(G, x, m, -L::cx(q), -L::cy(q), -L::cz(q));
-            B[idx] = Cvt<T>::from(v[q] * scale);
-        }
-    }
+    for (int q = 0; q < Q; ++q) g[q] = pdec<Q, T>(A[pull_index<Q>(G, x, m, q)], q);
 }
 
 // ------------------------------------------------------------------ ports
@@ -345,8 +259,9 @@ __device__ __forceinline__ Macro macroscopic(const float (&g)[Q], float alpha, c
     }
     M.rp = rp;
     M.rho = 1.f + rp;
-    const float inv_s = 1.f / (1.f + 0.5f * alpha);
-    const float inv_rho = 1.f / M.rho;
+    // approximate reciprocals (a few ulp; the FP32 state carries ~1e-7 anyway)
+    const float inv_s = __fdividef(1.f, 1.f + 0.5f * alpha);
+    const float inv_rho = __fdividef(1.f, M.rho);
     M.u[0] = (jx * inv_rho + 0.5f * P.a[0]) * inv_s;
     M.u[1] = (jy * inv_rho + 0.5f * P.a[1]) * inv_s;
     M.u[2] = (jz * inv_rho + 0.5f * P.a[2]) * inv_s;
@@ -365,105 +280,202 @@ __device__ __forceinline__ float dotc(int q, const float (&v)[3]) {
     return s;
 }
 
-// TRT collision in pair form (moving/collision.rs:457-488), in shifted
-// variables g = f - w; BGK is the case om == omega.  MRT adds the rank-one
-// corrections of the moments whose rate differs from the shear rate: the
-// odd moments of the Gram-Schmidt basis span exactly the antisymmetric
-// subspace, so MRT with all even rates equal to omega is TRT.
-template <int Q, int COLL>
-__device__ __forceinline__ void collide(float (&g)[Q], const Macro& M, const Physics& P) {
+// Pair sums s = v_i + v_opp(i), d = v_i - v_opp(i) feed the moments, the
+// TRT relaxation (moving/collision.rs:457-488, in pair form) and the mass
+// remainder in one pass.  SC = 0: v = g = f - w; SC = 1: v = (f - w)/w, the
+// 16-bit storage form, in which the weights drop out of the pair formulas.
+// Returns the macroscopic state of the loaded populations (implicit
+// half-step Brinkman velocity and Guo force, solver.rs:190-196); with
+// `post` the populations are replaced by their post-collision values.
+//
+// BGK is the case om == omega.  MRT adds one rank-one correction per even
+// moment whose rate differs from the shear rate: the odd moments of the
+// Gram-Schmidt basis span exactly the antisymmetric subspace, so MRT with
+// all even rates equal to omega is TRT.  The rest population takes the mass
+// remainder: the FP32 weights do not sum to one, which would otherwise leak
+// (rho - 1)(sum w - 1) per cell and step -- systematic where the pressure
+// has one sign.
+template <int Q, int COLL, int SC>
+__device__ __forceinline__ Macro collide_fused(float (&v)[Q], float alpha, const Physics& P, bool post) {
     using L = Lat<Q>;
+    constexpr int NP = L::NPAIR;
+    float S[NP], D[NP];
+    float rp = SC ? L::w(0) * v[0] : v[0];
+    float jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        const int i = k + 1, o = opp<Q>(i);
+        S[k] = v[i] + v[o];
+        D[k] = v[i] - v[o];
+        constexpr float one = 1.f;
+        const float w = SC ? L::w(i) : one;
+        rp = fmaf(w, S[k], rp);
+        if (L::cx(i)) jx = fmaf(w * L::cx(i), D[k], jx);
+        if (L::cy(i)) jy = fmaf(w * L::cy(i), D[k], jy);
+        if (L::cz(i)) jz = fmaf(w * L::cz(i), D[k], jz);
+    }
+    Macro M;
+    M.rp = rp;
+    M.rho = 1.f + rp;
+    // approximate reciprocals (a few ulp; the FP32 state carries ~1e-7 anyway)
+    const float inv_s = __fdividef(1.f, 1.f + 0.5f * alpha);
+    const float inv_rho = __fdividef(1.f, M.rho);
+    M.u[0] = (jx * inv_rho + 0.5f * P.a[0]) * inv_s;
+    M.u[1] = (jy * inv_rho + 0.5f * P.a[1]) * inv_s;
+    M.u[2] = (jz * inv_rho + 0.5f * P.a[2]) * inv_s;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) M.F[d] = M.rho * (P.a[d] - alpha * M.u[d]);
+    if (!post) return M;
+
     const float om = P.omega, omm = P.om;
     const float kp = 1.f - 0.5f * om, km = 1.f - 0.5f * omm;
-    const float* u = M.u;
-    const float* F = M.F;
-    const float usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-    const float uf = u[0] * F[0] + u[1] * F[1] + u[2] * F[2];
-    const float rho = M.rho, rp = M.rp;
+    const float hp = 0.5f * (1.f - om), hm = 0.5f * (1.f - omm);
+    const float rho = M.rho;
+    const float usq15 = 1.5f * (M.u[0] * M.u[0] + M.u[1] * M.u[1] + M.u[2] * M.u[2]);
+    const float uf3 = 3.f * (M.u[0] * M.F[0] + M.u[1] * M.F[1] + M.u[2] * M.F[2]);
     float dproj[MAX_PROJ];
     if constexpr (COLL == CK_MRT) {
+        // y = f - eq + src/2 of the rest population (g or g/w form)
+        const float w0 = SC ? 1.f : L::w(0);
+        const float y0 = v[0] - w0 * (rp - rho * usq15) - 0.5f * w0 * uf3;
 #pragma unroll
-        for (int p = 0; p < MAX_PROJ; ++p) dproj[p] = 0.f;
+        for (int p = 0; p < MAX_PROJ; ++p)
+            if (p < P.n_proj) dproj[p] = (SC ? L::w(0) : 1.f) * P.proj_right[p][0] * y0;
     }
-    {
-        const float w0 = L::w(0);
-        const float geq = w0 * (rp - 1.5f * rho * usq);
-        const float src = -3.f * w0 * uf;
-        if constexpr (COLL == CK_MRT) {
-            const float y0 = g[0] - geq + 0.5f * src;
+    float rem = rp;  // mass left for the rest population
+    if constexpr (COLL != CK_MRT) {
+        // Pair relaxation with the cell's constants folded:
+        //   P' = hp S + w [E0 + A cu^2 + 9 kp cu cf],  E0 = om (rp - rho 1.5 u^2) - kp 3 u.F,  A = 4.5 om rho
+        //   D' = hm D + w [G cu + 3 km cf],              G = 3 om_odd rho
+        // (the equilibrium and source terms of the MRT branch, regrouped).
+        const float E0 = fmaf(om, fmaf(-rho, usq15, rp), -kp * uf3);
+        const float A = 4.5f * om * rho, G = 3.f * omm * rho;
+        const float K9 = 9.f * kp, K3 = 3.f * km;
 #pragma unroll
-            for (int p = 0; p < MAX_PROJ; ++p)
-                if (p < P.n_proj) dproj[p] = fmaf(P.proj_right[p][0], y0, dproj[p]);
+        for (int k = 0; k < NP; ++k) {
+            const int i = k + 1, o = opp<Q>(i);
+            const float cu = dotc<Q>(i, M.u);
+            const float cf = dotc<Q>(i, M.F);
+            const float tp = fmaf(cu * cf, K9, fmaf(cu * cu, A, E0));
+            const float tm = fmaf(cu, G, cf * K3);
+            float Pp, Dm;
+            if constexpr (SC) {
+                Pp = fmaf(hp, S[k], tp);
+                Dm = fmaf(hm, D[k], tm);
+            } else {
+                Pp = fmaf(tp, L::w(i), hp * S[k]);
+                Dm = fmaf(tm, L::w(i), hm * D[k]);
+            }
+            v[i] = Pp + Dm;
+            v[o] = Pp - Dm;
+            rem = fmaf(SC ? -2.f * L::w(i) : -2.f, Pp, rem);
         }
-        g[0] = g[0] - om * (g[0] - geq) + kp * src;
-    }
+    } else {
 #pragma unroll
-    for (int i = 1; i <= L::NPAIR; ++i) {
-        const int o = opp<Q>(i);
-        const float w = L::w(i);
-        const float cu = dotc<Q>(i, M.u);
-        const float cf = dotc<Q>(i, M.F);
-        const float geqp = w * (rp + rho * (4.5f * cu * cu - 1.5f * usq));
-        const float eqm = 3.f * rho * w * cu;
-        const float sp = w * (9.f * cu * cf - 3.f * uf);
-        const float sm = 3.f * w * cf;
-        const float gp = 0.5f * (g[i] + g[o]);
-        const float gm = 0.5f * (g[i] - g[o]);
-        if constexpr (COLL == CK_MRT) {
-            const float yp = gp - geqp + 0.5f * sp;
+        for (int k = 0; k < NP; ++k) {
+            const int i = k + 1, o = opp<Q>(i);
+            const float w = SC ? 1.f : L::w(i);  // weight of the g form (1 in the g/w form)
+            const float cu = dotc<Q>(i, M.u);
+            const float cf = dotc<Q>(i, M.F);
+            const float geqp = w * fmaf(rho, fmaf(4.5f * cu, cu, -usq15), rp);  // symmetric part of eq
+            const float eqm = (3.f * w) * rho * cu;                             // antisymmetric part of eq
+            const float spv = w * fmaf(9.f * cu, cf, -uf3);                     // symmetric part of the source
+            const float smv = (3.f * w) * cf;                                   // antisymmetric part
+            float Pp = fmaf(hp, S[k], fmaf(kp, spv, om * geqp));
+            const float Dm = fmaf(hm, D[k], fmaf(km, smv, omm * eqm));
+            if constexpr (COLL == CK_MRT) {
+                const float yp = 0.5f * S[k] - geqp + 0.5f * spv;
 #pragma unroll
-            for (int p = 0; p < MAX_PROJ; ++p)
-                if (p < P.n_proj) dproj[p] = fmaf(2.f * P.proj_right[p][i], yp, dproj[p]);
+                for (int p = 0; p < MAX_PROJ; ++p)
+                    if (p < P.n_proj) dproj[p] = fmaf((SC ? 2.f * L::w(i) : 2.f) * P.proj_right[p][i], yp, dproj[p]);
+            }
+            v[i] = Pp + Dm;
+            v[o] = Pp - Dm;
+            rem = fmaf(SC ? -2.f * L::w(i) : -2.f, Pp, rem);
         }
-        const float A = kp * sp - om * (gp - geqp);
-        const float Bv = km * sm - omm * (gm - eqm);
-        g[i] = g[i] + A + Bv;
-        g[o] = g[o] + A - Bv;
-    }
-    if constexpr (COLL == CK_MRT) {
+        if constexpr (COLL == CK_MRT) {
 #pragma unroll
-        for (int p = 0; p < MAX_PROJ; ++p) {
-            if (p < P.n_proj) {
-                const float c = P.proj_rate[p] * dproj[p];
+            for (int p = 0; p < MAX_PROJ; ++p) {
+                if (p < P.n_proj) {
+                    const float c = P.proj_rate[p] * dproj[p];
 #pragma unroll
-                for (int i = 0; i < Q; ++i) g[i] = fmaf(-c, P.proj_left[p][i], g[i]);
+                    for (int k = 0; k < NP; ++k) {
+                        const int i = k + 1, o = opp<Q>(i);
+                        const float dv = c * (SC ? P.proj_lw[p][i] : P.proj_left[p][i]);
+                        v[i] -= dv;
+                        v[o] -= dv;
+                        rem = fmaf(SC ? 2.f * L::w(i) : 2.f, dv, rem);
+                    }
+                }
             }
         }
     }
-    // The collision conserves mass exactly; the FP32 weights do not sum to one,
-    // which would leak (rho - 1) * (sum w - 1) per cell and step -- systematic
-    // where the pressure has one sign.  The rest population takes the
-    // remainder, so only unbiased rounding remains.
-    float moving = 0.f;
-#pragma unroll
-    for (int i = 1; i < Q; ++i) moving += g[i];
-    g[0] = rp - moving;
+    v[0] = SC ? rem * (float)(1.0 / L::wd(0)) : rem;
+    return M;
 }
 
 // Collision transpose at the recorded (rho, u): given gb = d(loss)/d(post),
-// returns d(loss)/d(f) in gb and d(loss)/d(alpha).  Derivation: post = f - R y
-// + src, y = f - eq(rho, u) + src(u, F)/2; the cotangents of eq and src only
-// need the weighted zeroth, first and second moments of R^T gb, then the
+// returns d(loss)/d(f) in gb and d(loss)/d(alpha).  post = f - R y + src with
+// y = f - eq(rho, u) + src(u, F)/2; the cotangents of eq and src need only
+// the weighted zeroth, first and second moments of z = R^T gb and of
+// h = gb - z/2.  For TRT they are the moments of gb scaled by omega / om
+// (even / odd), taken pair by pair; the MRT rank-one terms add analytic
+// multiples of the precomputed moments of their basis vectors.  Then the
 // Brinkman chain F = rho (a - alpha u), u = (m/rho + a/2)/(1 + alpha/2).
 template <int Q, int COLL>
 __device__ __forceinline__ float collide_vjp(float (&gb)[Q], float rp, const float (&u)[3], float alpha,
                                              const Physics& P) {
     using L = Lat<Q>;
+    constexpr int NP = L::NPAIR;
     const float om = P.omega, omm = P.om;
     const float rho = 1.f + rp;
     const float s = 1.f + 0.5f * alpha;
     float F[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) F[d] = rho * (P.a[d] - alpha * u[d]);
-    // z = R^T gb
+    // weighted moments of gb and z = R^T gb (TRT part), pair by pair
+    float M0 = L::w(0) * gb[0];
+    float M1[3] = {0.f, 0.f, 0.f}, M2[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     float z[Q];
     z[0] = om * gb[0];
 #pragma unroll
-    for (int i = 1; i <= L::NPAIR; ++i) {
-        const int o = opp<Q>(i);
-        const float p = 0.5f * (gb[i] + gb[o]), mm = 0.5f * (gb[i] - gb[o]);
-        z[i] = om * p + omm * mm;
-        z[o] = om * p - omm * mm;
+    for (int k = 0; k < NP; ++k) {
+        const int i = k + 1, o = opp<Q>(i);
+        const float sm = gb[i] + gb[o], df = gb[i] - gb[o];
+        constexpr float half = 0.5f;
+        const float w = L::w(i);
+        const int c0 = L::cx(i), c1 = L::cy(i), c2 = L::cz(i);
+        M0 = fmaf(w, sm, M0);
+        if (c0) {
+            M1[0] = fmaf(w * c0, df, M1[0]);
+            M2[0] = fmaf(w, sm, M2[0]);
+        }
+        if (c1) {
+            M1[1] = fmaf(w * c1, df, M1[1]);
+            M2[1] = fmaf(w, sm, M2[1]);
+        }
+        if (c2) {
+            M1[2] = fmaf(w * c2, df, M1[2]);
+            M2[2] = fmaf(w, sm, M2[2]);
+        }
+        if (c0 && c1) M2[3] = fmaf(w * c0 * c1, sm, M2[3]);
+        if (c0 && c2) M2[4] = fmaf(w * c0 * c2, sm, M2[4]);
+        if (c1 && c2) M2[5] = fmaf(w * c1 * c2, sm, M2[5]);
+        const float a = half * om * sm, b = half * omm * df;
+        z[i] = a + b;
+        z[o] = a - b;
+    }
+    float Z0 = om * M0, H0 = (1.f - 0.5f * om) * M0;
+    float Z1[3], H1[3], Z2[6], H2[6];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        Z1[d] = omm * M1[d];
+        H1[d] = (1.f - 0.5f * omm) * M1[d];
+    }
+#pragma unroll
+    for (int e = 0; e < 6; ++e) {
+        Z2[e] = om * M2[e];
+        H2[e] = (1.f - 0.5f * om) * M2[e];
     }
     if constexpr (COLL == CK_MRT) {
 #pragma unroll
@@ -475,29 +487,15 @@ __device__ __forceinline__ float collide_vjp(float (&gb)[Q], float rp, const flo
                 const float c = P.proj_rate[p] * e;
 #pragma unroll
                 for (int i = 0; i < Q; ++i) z[i] = fmaf(c, P.proj_right[p][i], z[i]);
+                Z0 = fmaf(c, P.proj_m0[p], Z0);
+                H0 = fmaf(-0.5f * c, P.proj_m0[p], H0);
+#pragma unroll
+                for (int e2 = 0; e2 < 6; ++e2) {
+                    Z2[e2] = fmaf(c, P.proj_m2[p][e2], Z2[e2]);
+                    H2[e2] = fmaf(-0.5f * c, P.proj_m2[p][e2], H2[e2]);
+                }
             }
         }
-    }
-    // weighted moments of z and of h = gb - z/2
-    float Z0 = 0.f, Z1[3] = {0.f, 0.f, 0.f}, Z2[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    float H0 = 0.f, H1[3] = {0.f, 0.f, 0.f}, H2[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        const float w = L::w(i);
-        const float zw = w * z[i];
-        const float hw = w * (gb[i] - 0.5f * z[i]);
-        const int c0 = L::cx(i), c1 = L::cy(i), c2 = L::cz(i);
-        Z0 += zw;
-        H0 += hw;
-        if (c0) { Z1[0] += c0 * zw; H1[0] += c0 * hw; }
-        if (c1) { Z1[1] += c1 * zw; H1[1] += c1 * hw; }
-        if (c2) { Z1[2] += c2 * zw; H1[2] += c2 * hw; }
-        if (c0) { Z2[0] += zw; H2[0] += hw; }
-        if (c1) { Z2[1] += zw; H2[1] += hw; }
-        if (c2) { Z2[2] += zw; H2[2] += hw; }
-        if (c0 && c1) { Z2[3] += c0 * c1 * zw; H2[3] += c0 * c1 * hw; }
-        if (c0 && c2) { Z2[4] += c0 * c2 * zw; H2[4] += c0 * c2 * hw; }
-        if (c1 && c2) { Z2[5] += c1 * c2 * zw; H2[5] += c1 * c2 * hw; }
     }
     // Z2 u, H2 u, H2 F (symmetric 3x3 stored xx yy zz xy xz yz)
     auto mul = [](const float (&S)[6], const float* v, float* out) {
@@ -525,14 +523,15 @@ __device__ __forceinline__ float collide_vjp(float (&gb)[Q], float rp, const flo
         abar -= rho * Fb[d] * u[d];
         ub[d] -= rho * alpha * Fb[d];
     }
-    const float inv = 1.f / (s * rho);
+    const float inv_s = __fdividef(1.f, s);
+    const float inv = __fdividef(inv_s, rho);
     float mb[3];
     float sbar = 0.f;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         mb[d] = ub[d] * inv;
         rho_bar -= ub[d] * (s * u[d] - 0.5f * P.a[d]) * inv;
-        sbar -= ub[d] * u[d] / s;
+        sbar -= ub[d] * u[d] * inv_s;
     }
     abar += 0.5f * sbar;
 #pragma unroll
@@ -831,8 +830,9 @@ namespace {
 // run's misalignment.  Blocked links (walls, solids) and cells on periodic
 // faces read their few populations from global memory directly.
 constexpr int CONSUMER_WARPS = 8;
-constexpr int TILE = CONSUMER_WARPS * 32;
-constexpr int TPB = TILE + 32;
+constexpr int CPT = 1;                         // cells per consumer thread and tile
+constexpr int TILE = CONSUMER_WARPS * 32 * CPT;
+constexpr int TPB = CONSUMER_WARPS * 32 + 32;
 constexpr int STAGES = 3;
 
 template <typename T>
@@ -857,63 +857,21 @@ __device__ __forceinline__ S* stage_at(unsigned char* smem, int s) {
     return reinterpret_cast<S*>(smem + 128 + s * stage_stride<S>());
 }
 
-// Forward AA store with the parity known at compile time.
-template <int Q, typename T, int PAR>
-__device__ __forceinline__ void store_pop_p(T* A, const Geometry& G, uint32_t x, uint32_t m, const float (&g)[Q],
-                                            uint32_t step) {
-    using L = Lat<Q>;
-    const uint32_t n = (uint32_t)G.n;
+// Aligned store of one cell's values into its own slots of the output array
+// (populations in storage units with stochastic rounding for 16-bit storage,
+// or adjoint values scaled by `scale`).
+template <int Q, typename T>
+__device__ __forceinline__ void store_own_pop(T* A, uint32_t n, uint32_t x, const float (&v)[Q], uint32_t step) {
     uint32_t rs = 0;
     if constexpr (Cvt<T>::scaled) rs = cell_seed(x, step);
-    if constexpr (PAR == 0) {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) A[opp<Q>(q) * n + x] = penc_sr<Q, T>(g[q], q, rs);
-    } else {
-        if (!(m & MASK_WRAP)) {
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const uint32_t own = opp<Q>(q) * n + x;
-                const uint32_t nb = q * n + x + lin<Q>(G, q, +1);
-                A[((m >> opp<Q>(q)) & 1u) ? own : nb] = penc_sr<Q, T>(g[q], q, rs);
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                uint32_t idx;
-                if (m & (1u << opp<Q>(q))) idx = opp<Q>(q) * n + x;
-                else idx = q * n + neighbor(G, x, m, L::cx(q), L::cy(q), L::cz(q));
-                A[idx] = penc_sr<Q, T>(g[q], q, rs);
-            }
-        }
-    }
+    for (int q = 0; q < Q; ++q) A[q * n + x] = senc_sr<T>(v[q], rs);
 }
 
-template <int Q, typename T, int PAR>
-__device__ __forceinline__ void store_lam_p(T* B, const Geometry& G, uint32_t x, uint32_t m, float scale,
-                                            const float (&v)[Q]) {
-    using L = Lat<Q>;
-    const uint32_t n = (uint32_t)G.n;
-    if constexpr (PAR == 0) {
+template <int Q, typename T>
+__device__ __forceinline__ void store_own_lam(T* B, uint32_t n, uint32_t x, const float (&v)[Q], float scale) {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) B[opp<Q>(q) * n + x] = Cvt<T>::from(v[q] * scale);
-    } else {
-        if (!(m & MASK_WRAP)) {
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const uint32_t own = opp<Q>(q) * n + x;
-                const uint32_t nb = q * n + x + lin<Q>(G, q, -1);
-                B[((m >> q) & 1u) ? own : nb] = Cvt<T>::from(v[q] * scale);
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                uint32_t idx;
-                if (m & (1u << q)) idx = opp<Q>(q) * n + x;
-                else idx = q * n + neighbor(G, x, m, -L::cx(q), -L::cy(q), -L::cz(q));
-                B[idx] = Cvt<T>::from(v[q] * scale);
-            }
-        }
-    }
+    for (int q = 0; q < Q; ++q) B[q * n + x] = Cvt<T>::from(v[q] * scale);
 }
 
 template <typename K>

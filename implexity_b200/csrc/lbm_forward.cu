@@ -1,11 +1,15 @@
-// lbm_forward.cu -- the fused collide-stream step (AA pattern, in place).
+// lbm_forward.cu -- the fused stream-collide step (pull, two arrays).
 //
-// One launch = one time step of the whole grid: load (AA parity) -> port
-// reconstruction (ports.rs:560-579) -> admission reductions of the loaded
+// One launch = one time step of the whole grid: pull from the current array
+// (Streaming::stream with halfway bounce-back, solver.rs:131-157) -> port
+// reconstruction (ports.rs:560-579) -> admission reductions of the streamed
 // state (solver.rs:714-755) -> optional (rho, u) record for the adjoint ->
-// collision (BGK/TRT/MRT with Guo-Brinkman forcing) -> AA store.  The loads
-// are staged through shared memory by a producer warp (bulk asynchronous
-// copies into a STAGES-deep ring); see lbm_device.cuh.
+// collision (BGK/TRT/MRT with Guo-Brinkman forcing) -> aligned store into the
+// cell's own slots of the other array.  The pulled runs are staged through
+// shared memory by a producer warp (bulk asynchronous copies into a
+// STAGES-deep ring); see lbm_device.cuh.  Reading one array and writing
+// another keeps every DRAM stream one-directional, which on this memory
+// system sustains about a third more bandwidth than the in-place AA pattern.
 #include "lbm_device.cuh"
 
 namespace lbm {
@@ -18,17 +22,24 @@ struct FwdStage {
     float alpha[FRUN];
 };
 
-template <int Q, int COLL, typename T, int PAR>
+template <int Q, int COLL, typename T>
 __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
     using L = Lat<Q>;
     using S = FwdStage<Q, T>;
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem);
-    uint64_t* empty = full + STAGES;
-    T* A = static_cast<T*>(a.pop);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem);  // stage loaded
+    uint64_t* empty = full + STAGES;                      // stage consumed (outputs written into it)
+    uint64_t* rdone = empty + STAGES;                     // stage inputs read by every consumer warp
+    const T* A = static_cast<const T*>(a.src);
+    T* D = static_cast<T*>(a.dst);
     const uint32_t n = (uint32_t)a.G.n;
     const uint32_t ntiles = (n + TILE - 1) / TILE;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // Outputs of a full tile leave through the stage: every consumer writes
+    // its cell's values into the aligned head of each run once all warps have
+    // read the stage, and the producer copies the Q runs to the cells' own
+    // slots with bulk stores.  The last, partial tile stores directly.
+    const bool bulk_ok = a.collide && a.bulk_store;
     DiagLocal acc;
     acc.init();
     if (threadIdx.x == 0) {
@@ -36,78 +47,131 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], CONSUMER_WARPS);
+            mbar_init(&rdone[s], CONSUMER_WARPS);
         }
         mbar_fence_init();
     }
     __syncthreads();
     if (warp == 0) {
-        // producer: one lane issues the runs of every tile of this block
-        if (lane == 0) {
-            int s = 0;
-            uint32_t round = 0;  // completed passes over the ring
-            for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-                if (round > 0 && !mbar_wait(&empty[s], (round - 1) & 1u, a.err)) break;
-                S* st = stage_at<S>(smem, s);
-                const uint32_t x0 = tile * TILE;
-                mbar_expect_tx(&full[s], Q * Vec16<T>::BYTES + 2 * FRUN_BYTES);
+        // producer warp: lane q issues the copy of direction q's run (lanes Q, Q+1
+        // the mask and alpha runs), so a tile's copies leave in one instruction
+        const uint32_t mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+        const int q = lane < Q ? lane : 0;
+        const int64_t run0 = a.run0[q];
 #pragma unroll 1
-                for (int q = 0; q < Q; ++q) bulk_g2s(&st->run[q][0], A + (a.run0[q] + x0), Vec16<T>::BYTES, &full[s]);
-                bulk_g2s(&st->mask[0], a.mask + x0, FRUN_BYTES, &full[s]);
-                bulk_g2s(&st->alpha[0], a.alpha + x0, FRUN_BYTES, &full[s]);
-                if (++s == STAGES) {
-                    s = 0;
-                    ++round;
+        for (uint32_t i = 0; i < mine + STAGES; ++i) {
+            const int s = (int)(i % STAGES);
+            const uint32_t round = i / STAGES;
+            S* st = stage_at<S>(smem, s);
+            if (round > 0) {
+                // the tile loaded STAGES iterations ago is consumed; store it
+                // (lane 0 waits; the whole warp leaves together on a timeout)
+                bool done = true;
+                if (lane == 0) done = mbar_wait(&empty[s], (round - 1) & 1u, a.err);
+                if (!__shfl_sync(0xffffffffu, done, 0)) break;
+                const uint32_t x0 = (blockIdx.x + (i - STAGES) * gridDim.x) * TILE;
+                if (bulk_ok && x0 + TILE <= n) {
+                    if (lane < Q) {
+                        bulk_s2g(D + ((size_t)lane * n + x0), &st->run[lane][0], TILE * (int)sizeof(T));
+                        bulk_commit();
+                        bulk_wait_read0();  // the stage may be refilled once the stores have read it
+                    }
+                    __syncwarp();
                 }
             }
+            if (i < mine) {
+                const uint32_t x0 = (blockIdx.x + i * gridDim.x) * TILE;
+                if (lane == 0) mbar_expect_tx(&full[s], Q * Vec16<T>::BYTES + 2 * FRUN_BYTES);
+                __syncwarp();
+                if (lane < Q) bulk_g2s(&st->run[lane][0], A + (run0 + x0), Vec16<T>::BYTES, &full[s]);
+                else if (lane == Q) bulk_g2s(&st->mask[0], a.mask + x0, FRUN_BYTES, &full[s]);
+                else if (lane == Q + 1) bulk_g2s(&st->alpha[0], a.alpha + x0, FRUN_BYTES, &full[s]);
+            }
         }
+        bulk_wait_all();
     } else {
         const int c = threadIdx.x - 32;
         int s = 0;
         uint32_t round = 0;
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
             const bool ok = mbar_wait(&full[s], round & 1u, a.err);
-            const S* st = stage_at<S>(smem, s);
+            S* st = stage_at<S>(smem, s);
             const uint32_t x = tile * TILE + c;
-            if (ok && x < n) {
-                const uint32_t m = st->mask[c];
-                if (!(m & MASK_SOLID)) {
-                    float g[Q];
-                    if (PAR == 0 || !(m & MASK_WRAP)) {
+            const bool bulk = bulk_ok && tile * TILE + TILE <= n;
+            // populations in storage units (g = f - w, or (f - w)/w for 16-bit storage)
+            constexpr int SC = Cvt<T>::scaled ? 1 : 0;
+            float v[Q];
+            const uint32_t m = ok && x < n ? st->mask[c] : MASK_SOLID;
+            const bool fluid = !(m & MASK_SOLID);
+            if (fluid) {
+                if (!(m & MASK_WRAP)) {
 #pragma unroll
-                        for (int q = 0; q < Q; ++q) {
-                            if (PAR == 1 && ((m >> q) & 1u)) g[q] = pdec<Q, T>(A[q * n + x], q);
-                            else g[q] = pdec<Q, T>(st->run[q][a.rund[q] + c], q);
-                        }
-                    } else {
-                        load_pop<Q, T>(A, a.G, x, m, PAR, g);
-                    }
-                    float exch = 0.f;
-                    if (a.apply_ports && (m & MASK_PORT))
-                        exch = apply_port<Q>(a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], g);
-                    const float alpha = st->alpha[c];
-                    Macro M = macroscopic<Q>(g, alpha, a.P);
-                    if (a.diag) {
-                        acc.mass += M.rp;
-                        acc.exch += exch;
-                        float mn = INFINITY;
+                    for (int q = 0; q < Q; ++q) v[q] = sdec<T>(st->run[q][a.rund[q] + c]);
+                    if (m & LINK_BITS) {
+                        // halfway bounce-back: the cell's own opposite slot
 #pragma unroll
-                        for (int q = 0; q < Q; ++q) mn = fminf(mn, L::w(q) + g[q]);
-                        acc.minf = fminf(acc.minf, mn);
-                        acc.maxu2 = fmaxf(acc.maxu2, M.u[0] * M.u[0] + M.u[1] * M.u[1] + M.u[2] * M.u[2]);
-                        // any non-finite population makes the density sum non-finite
-                        if (!isfinite(M.rp)) acc.nf = 1;
+                        for (int q = 1; q < Q; ++q)
+                            if ((m >> q) & 1u) v[q] = sdec<T>(A[opp<Q>(q) * n + x]);
                     }
-                    if (a.record) {
-                        a.record[x] = M.rp;
-                        a.record[n + x] = M.u[0];
-                        a.record[2 * n + x] = M.u[1];
-                        a.record[3 * n + x] = M.u[2];
+                } else {
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) v[q] = sdec<T>(A[pull_index<Q>(a.G, x, m, q)]);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&rdone[s]);
+            if (fluid) {
+                const float alpha = st->alpha[c];
+                float exch = 0.f;
+                if (a.apply_ports && (m & MASK_PORT)) {
+                    // the port maps act on g = f - w
+                    if constexpr (SC) {
+#pragma unroll
+                        for (int q = 0; q < Q; ++q) v[q] *= L::w(q);
                     }
-                    if (a.collide) {
-                        collide<Q, COLL>(g, M, a.P);
-                        store_pop_p<Q, T, PAR>(A, a.G, x, m, g, a.step);
+                    exch = apply_port<Q>(a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], v);
+                    if constexpr (SC) {
+#pragma unroll
+                        for (int q = 0; q < Q; ++q) v[q] *= (float)(1.0 / L::wd(q));
                     }
                 }
+                float mn = INFINITY;
+                if (a.diag) {
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) mn = fminf(mn, SC ? L::w(q) * (1.f + v[q]) : L::w(q) + v[q]);
+                }
+                const Macro M = collide_fused<Q, COLL, SC>(v, alpha, a.P, a.collide);
+                if (a.diag) {
+                    acc.mass += M.rp;
+                    acc.exch += exch;
+                    acc.minf = fminf(acc.minf, mn);
+                    acc.maxu2 = fmaxf(acc.maxu2, M.u[0] * M.u[0] + M.u[1] * M.u[1] + M.u[2] * M.u[2]);
+                    // any non-finite population makes the density sum non-finite
+                    if (!isfinite(M.rp)) acc.nf = 1;
+                }
+                if (a.record) {
+                    a.record[x] = M.rp;
+                    a.record[n + x] = M.u[0];
+                    a.record[2 * n + x] = M.u[1];
+                    a.record[3 * n + x] = M.u[2];
+                }
+                if (a.collide && !bulk) store_own_pop<Q, T>(D, n, x, v, a.step);
+            }
+            if (bulk) {
+                // every warp has read its inputs: overwrite the run heads with this cell's outputs
+                // (a solid cell carries its held populations over)
+                if (!mbar_wait(&rdone[s], round & 1u, a.err)) {
+                    // nothing is stored for this tile; the error flag fails the step
+                } else if (fluid) {
+                    uint32_t rs = 0;
+                    if constexpr (Cvt<T>::scaled) rs = cell_seed(x, a.step);
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) st->run[q][c] = senc_sr<T>(v[q], rs);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) st->run[q][c] = A[q * n + x];
+                }
+                fence_proxy_async_smem();
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);
@@ -120,39 +184,28 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
     if (a.diag) finish_diag(acc, a.diag, a.red);
 }
 
-template <int Q, int COLL, typename T, int PAR>
+template <int Q, int COLL, typename T>
 cudaError_t run_forward(const FwdArgs& a, cudaStream_t s) {
     constexpr size_t smem = pipe_bytes<FwdStage<Q, T>>();
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = set_smem(k_forward<Q, COLL, T, PAR>, smem);
+        cudaError_t e = set_smem(k_forward<Q, COLL, T>, smem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    const int grid = persistent_grid((const void*)k_forward<Q, COLL, T, PAR>, a.G.n, smem, TPB, TILE);
-    k_forward<Q, COLL, T, PAR><<<grid, TPB, smem, s>>>(a);
+    const int grid = persistent_grid((const void*)k_forward<Q, COLL, T>, a.G.n, smem, TPB, TILE);
+    k_forward<Q, COLL, T><<<grid, TPB, smem, s>>>(a);
     return cudaGetLastError();
-}
-
-template <int Q, int COLL, typename T>
-cudaError_t run_forward_p(const FwdArgs& a, cudaStream_t s) {
-    return a.parity == 0 ? run_forward<Q, COLL, T, 0>(a, s) : run_forward<Q, COLL, T, 1>(a, s);
 }
 
 }  // namespace
 
-void run_table(int Q, const Geometry& G, int parity, int dir, int vec, int64_t* run0, int32_t* rund) {
+void run_table(int Q, const Geometry& G, int dir, int vec, int64_t* run0, int32_t* rund) {
     for (int q = 0; q < Q; ++q) {
-        int64_t first;
-        if (parity == 0) {
-            first = (int64_t)q * G.n;
-        } else {
-            const int cx = Q == 19 ? Lat<19>::cx(q) : Lat<27>::cx(q);
-            const int cy = Q == 19 ? Lat<19>::cy(q) : Lat<27>::cy(q);
-            const int cz = Q == 19 ? Lat<19>::cz(q) : Lat<27>::cz(q);
-            const int o = q == 0 ? 0 : Q - q;
-            first = (int64_t)o * G.n + dir * (cx * G.sx + cy * G.sy + cz);
-        }
+        const int cx = Q == 19 ? Lat<19>::cx(q) : Lat<27>::cx(q);
+        const int cy = Q == 19 ? Lat<19>::cy(q) : Lat<27>::cy(q);
+        const int cz = Q == 19 ? Lat<19>::cz(q) : Lat<27>::cz(q);
+        const int64_t first = (int64_t)q * G.n + dir * (cx * G.sx + cy * G.sy + cz);
         int64_t d = first % vec;
         if (d < 0) d += vec;
         run0[q] = first - d;
@@ -163,18 +216,18 @@ void run_table(int Q, const Geometry& G, int parity, int dir, int vec, int64_t* 
 cudaError_t launch_forward(int Q, int coll, int storage, const FwdArgs& a0, int grid, cudaStream_t s) {
     (void)grid;
     FwdArgs a = a0;
-    run_table(Q, a.G, a.parity, -1, storage == ST_F32 ? 4 : 8, a.run0, a.rund);
+    run_table(Q, a.G, -1, storage == ST_F32 ? 4 : 8, a.run0, a.rund);
     if (Q == 19) {
         if (coll == CK_MRT) {
-            LBM_STORAGE_DISPATCH(storage, T, return run_forward_p<19, CK_MRT, T>(a, s))
+            LBM_STORAGE_DISPATCH(storage, T, return run_forward<19, CK_MRT, T>(a, s))
         } else {
-            LBM_STORAGE_DISPATCH(storage, T, return run_forward_p<19, CK_PAIRS, T>(a, s))
+            LBM_STORAGE_DISPATCH(storage, T, return run_forward<19, CK_PAIRS, T>(a, s))
         }
     } else {
         if (coll == CK_MRT) {
-            LBM_STORAGE_DISPATCH(storage, T, return run_forward_p<27, CK_MRT, T>(a, s))
+            LBM_STORAGE_DISPATCH(storage, T, return run_forward<27, CK_MRT, T>(a, s))
         } else {
-            LBM_STORAGE_DISPATCH(storage, T, return run_forward_p<27, CK_PAIRS, T>(a, s))
+            LBM_STORAGE_DISPATCH(storage, T, return run_forward<27, CK_PAIRS, T>(a, s))
         }
     }
     return cudaGetLastError();

@@ -8,11 +8,12 @@
 
 namespace lbm {
 
-// Population storage.  F32 stores g = f - w; F16/BF16 store g/w.  Population
-// and adjoint arrays carry pop_pad(G) elements of padding before plane 0 and
-// after the last plane (the staged runs of the stepping kernels read a little
-// outside the planes); per-cell float/uint arrays carry CELL_PAD elements
-// after the last cell.
+// Population storage.  F32 stores g = f - w; F16/BF16 store g/w.  The state
+// and the adjoint each live in two arrays (the step reads one and writes the
+// other).  Every array carries pop_pad(G) elements of padding before plane 0
+// and after the last plane (the staged runs of the stepping kernels read a
+// little outside the planes); per-cell float/uint arrays carry CELL_PAD
+// elements after the last cell.
 constexpr int64_t CELL_PAD = 1024;
 inline int64_t pop_pad(const Geometry& G) { return ((G.sx + G.sy + 1 + 2 * CELL_PAD) + 63) / 64 * 64; }
 enum StoreKind { ST_F32 = 0, ST_F16 = 1, ST_BF16 = 2 };
@@ -21,21 +22,22 @@ enum CollKind { CK_PAIRS = 0, CK_MRT = 1 };  // BGK runs as PAIRS with om == ome
 struct FwdArgs {
     Geometry G;
     Physics P;
-    void* pop;               // Q planes of n cells (storage type)
+    const void* src;         // current array: Q planes of n cells (storage type)
+    void* dst;               // output array of the step
     const uint32_t* mask;
     const float* alpha;
     const PortMap* ports;
-    int32_t parity;          // 0: in-place swap step, 1: neighbour step
     int32_t apply_ports;     // the stored state still needs the port reconstruction
     StepDiag* diag;          // per-state admission output (nullptr: off)
     Reduce red;
     float* record;           // (rho-1, ux, uy, uz) planes (nullptr: off)
     int32_t collide;         // 0: only load/diag/record (no collision, no store)
+    int32_t bulk_store;      // full tiles leave through bulk stores (planes 16-byte aligned)
     uint32_t step;           // absolute step index (seeds the stochastic rounding)
     int* err;                // set when a bounded wait gave up
-    // staged runs of this step's parity: element offset of each direction's
-    // 16-byte aligned run for the tile at x0 = 0, and the offset of the
-    // tile's first element inside it
+    // staged pull runs: element offset of each direction's 16-byte aligned
+    // run for the tile at x0 = 0, and the offset of the tile's first element
+    // inside it
     int64_t run0[27];
     int32_t rund[27];
 };
@@ -43,13 +45,13 @@ struct FwdArgs {
 struct AdjArgs {
     Geometry G;
     Physics P;
-    void* lam;               // Q planes of n cells (lambda storage type)
+    const void* src;         // current adjoint array: Q planes of n cells (lambda storage type)
+    void* dst;               // output array of the transposed step
     const uint32_t* mask;
     const float* alpha;
     const PortMap* ports;
     const float* record;     // (rho-1, ux, uy, uz) of the forward state
     float* abar;             // accumulated alpha cotangent
-    int32_t parity;
     int32_t port_transpose;  // store Ports^T lambda (1) or lambda itself (0)
     int32_t overwrite_abar;  // abar = (1) or += (0)
     float in_scale_inv;      // true = stored * in_scale_inv
@@ -72,7 +74,6 @@ struct ObjArgs {
     const float* alpha;
     const float* phi;
     const PortMap* ports;
-    int32_t parity;
     int32_t apply_ports;
     float tau;
     // response scales
@@ -116,9 +117,9 @@ struct DesignArgs {
 };
 
 // Fills run0/rund for a tile-staged kernel: direction q's run starts at the
-// first used element q*n + x0 (parity 0) or opp(q)*n + x0 + dir*lin(q)
-// (parity 1), aligned down to `vec` elements.
-void run_table(int Q, const Geometry& G, int parity, int dir, int vec, int64_t* run0, int32_t* rund);
+// first used element q*n + x0 + dir*lin(q) (dir -1: forward pull, +1:
+// adjoint pull), aligned down to `vec` elements.
+void run_table(int Q, const Geometry& G, int dir, int vec, int64_t* run0, int32_t* rund);
 
 // Sets the message lbm_last_error(NULL) returns on this thread (entry points
 // that take no handle report through it).
@@ -131,12 +132,11 @@ cudaError_t launch_adjoint(int Q, int coll, int lstorage, const AdjArgs& a, int 
 cudaError_t launch_objective(int Q, int storage, int lstorage, int mode, const ObjArgs& a, int grid,
                              cudaStream_t s);  // mode 0: responses/fields, 1: seed
 cudaError_t launch_canon_pop(int Q, int storage, const Geometry& G, const void* pop, const uint32_t* mask,
-                             const PortMap* ports, int parity, int apply_ports, float* out, int grid,
-                             cudaStream_t s);
-cudaError_t launch_upload_pop(int Q, int storage, const Geometry& G, void* pop, const float* in, int grid,
-                              cudaStream_t s);
+                             const PortMap* ports, int apply_ports, float* out, int grid, cudaStream_t s);
+cudaError_t launch_upload_pop(int Q, int storage, const Geometry& G, void* pop, const uint32_t* mask,
+                              const float* in, int grid, cudaStream_t s);
 cudaError_t launch_canon_lam(int Q, int lstorage, const Geometry& G, const void* lam, const uint32_t* mask,
-                             int after_odd, float inv_scale, float* out, int grid, cudaStream_t s);
+                             float inv_scale, float* out, int grid, cudaStream_t s);
 cudaError_t launch_seed_lam(int Q, int lstorage, const Geometry& G, void* lam, const uint32_t* mask,
                             const PortMap* ports, const float* in, float scale, int port_transpose, int grid,
                             cudaStream_t s);

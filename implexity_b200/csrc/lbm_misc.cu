@@ -1,23 +1,29 @@
 // lbm_misc.cu -- one-off kernels around the stepping: initial state,
 // responses and their VJP (the adjoint seed), state/adjoint layout
-// conversions, the design map and its transpose.
+// conversions, the design map and its transpose.  Streamed states are read
+// through the pull of the stepping kernels and written through its inverse
+// scatter (pull_index, lbm_device.cuh).
 #include "lbm_device.cuh"
 
 namespace lbm {
 namespace {
 
 // ------------------------------------------------------------------ kernels
+// Initial streamed state (initial_populations, solver.rs:593-601): fluid
+// w(1 - 1.5 c.a), solid w.  Fluid cells scatter through the inverse pull,
+// solid cells fill their own slots.
 template <int Q, typename T>
 __global__ void __launch_bounds__(BLOCK) k_init(Geometry G, Physics P, T* A, const uint32_t* __restrict__ mask) {
     using L = Lat<Q>;
-    for (int64_t x = (int64_t)blockIdx.x * BLOCK + threadIdx.x; x < G.n; x += (int64_t)gridDim.x * BLOCK) {
-        const bool solid = mask[x] & MASK_SOLID;
+    const uint32_t n = (uint32_t)G.n;
+    for (uint32_t x = blockIdx.x * BLOCK + threadIdx.x; x < n; x += gridDim.x * BLOCK) {
+        const uint32_t m = mask[x];
+        const bool solid = m & MASK_SOLID;
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            // initial_populations, solver.rs:593-601: fluid w(1 - 1.5 c.a), solid w
             const float ca = L::cx(q) * P.a[0] + L::cy(q) * P.a[1] + L::cz(q) * P.a[2];
             const float g = solid ? 0.f : -1.5f * L::w(q) * ca;
-            A[(int64_t)q * G.n + x] = penc<Q, T>(g, q);
+            A[solid ? q * n + x : pull_index<Q>(G, x, m, q)] = penc<Q, T>(g, q);
         }
     }
 }
@@ -47,7 +53,7 @@ __global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
             continue;
         }
         float g[Q];
-        load_pop<Q, T>(A, a.G, x, m, a.parity, g);
+        load_pop<Q, T>(A, a.G, x, m, g);
         const PortMap* pm = (m & MASK_PORT) ? &a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1] : nullptr;
         if (a.apply_ports && pm) apply_port<Q>(*pm, g);
         const float alpha = a.alpha[x];
@@ -173,7 +179,7 @@ __global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
             if (a.write_lambda) {
                 TL* B = static_cast<TL*>(a.lam);
 #pragma unroll
-                for (int q = 0; q < Q; ++q) B[opp<Q>(q) * n + x] = Cvt<TL>::from(fb[q] * a.lam_scale);
+                for (int q = 0; q < Q; ++q) B[q * n + x] = Cvt<TL>::from(fb[q] * a.lam_scale);
             }
             if (a.norm2) {
 #pragma unroll
@@ -196,9 +202,10 @@ __global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
     }
 }
 
+// Streamed state (with the pending port reconstruction) in natural planes.
 template <int Q, typename T>
 __global__ void __launch_bounds__(BLOCK) k_canon_pop(Geometry G, const T* A, const uint32_t* __restrict__ mask,
-                                                     const PortMap* ports, int parity, int apply_ports, float* out) {
+                                                     const PortMap* ports, int apply_ports, float* out) {
     for (uint32_t x = blockIdx.x * BLOCK + threadIdx.x; x < (uint32_t)G.n; x += gridDim.x * BLOCK) {
         const uint32_t m = mask[x];
         float g[Q];
@@ -206,7 +213,7 @@ __global__ void __launch_bounds__(BLOCK) k_canon_pop(Geometry G, const T* A, con
 #pragma unroll
             for (int q = 0; q < Q; ++q) g[q] = pdec<Q, T>(A[(int64_t)q * G.n + x], q);
         } else {
-            load_pop<Q, T>(A, G, x, m, parity, g);
+            load_pop<Q, T>(A, G, x, m, g);
             if (apply_ports && (m & MASK_PORT)) apply_port<Q>(ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], g);
         }
 #pragma unroll
@@ -214,34 +221,29 @@ __global__ void __launch_bounds__(BLOCK) k_canon_pop(Geometry G, const T* A, con
     }
 }
 
+// A given streamed state (natural planes, g = f - w) -> stored layout: the
+// inverse of the pull for fluid cells, own slots for solid cells.
 template <int Q, typename T>
-__global__ void __launch_bounds__(BLOCK) k_upload_pop(Geometry G, T* A, const float* in) {
-    for (int64_t x = (int64_t)blockIdx.x * BLOCK + threadIdx.x; x < G.n; x += (int64_t)gridDim.x * BLOCK) {
+__global__ void __launch_bounds__(BLOCK) k_upload_pop(Geometry G, T* A, const uint32_t* __restrict__ mask,
+                                                      const float* in) {
+    const uint32_t n = (uint32_t)G.n;
+    for (uint32_t x = blockIdx.x * BLOCK + threadIdx.x; x < n; x += gridDim.x * BLOCK) {
+        const uint32_t m = mask[x];
 #pragma unroll
-        for (int q = 0; q < Q; ++q) A[(int64_t)q * G.n + x] = penc<Q, T>(in[(int64_t)q * G.n + x], q);
+        for (int q = 0; q < Q; ++q)
+            A[(m & MASK_SOLID) ? q * n + x : pull_index<Q>(G, x, m, q)] = penc<Q, T>(in[(size_t)q * n + x], q);
     }
 }
 
-// Natural-order lambda after an adjoint step (after_odd) or after a seed /
-// parity-0 adjoint step.
+// Natural-order lambda after a transposed step (own slots; zero at solids).
 template <int Q, typename T>
 __global__ void __launch_bounds__(BLOCK) k_canon_lam(Geometry G, const T* B, const uint32_t* __restrict__ mask,
-                                                     int after_odd, float inv_scale, float* out) {
-    using L = Lat<Q>;
+                                                     float inv_scale, float* out) {
     for (int64_t x = (int64_t)blockIdx.x * BLOCK + threadIdx.x; x < G.n; x += (int64_t)gridDim.x * BLOCK) {
-        const uint32_t m = mask[x];
+        const bool solid = mask[x] & MASK_SOLID;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            float v = 0.f;
-            if (!(m & MASK_SOLID)) {
-                const uint32_t n = (uint32_t)G.n;
-                uint32_t idx;
-                if (!after_odd || (m & (1u << q))) idx = opp<Q>(q) * n + (uint32_t)x;
-                else idx = q * n + neighbor(G, (uint32_t)x, m, -L::cx(q), -L::cy(q), -L::cz(q));
-                v = Cvt<T>::to(B[idx]) * inv_scale;
-            }
-            out[(int64_t)q * G.n + x] = v;
-        }
+        for (int q = 0; q < Q; ++q)
+            out[(int64_t)q * G.n + x] = solid ? 0.f : Cvt<T>::to(B[(int64_t)q * G.n + x]) * inv_scale;
     }
 }
 
@@ -258,7 +260,7 @@ __global__ void __launch_bounds__(BLOCK) k_seed_lam(Geometry G, T* B, const uint
         for (int q = 0; q < Q; ++q) v[q] = in[(int64_t)q * G.n + x];
         if (port_transpose_on && (m & MASK_PORT)) port_transpose<Q>(ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], v);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) B[opp<Q>(q) * G.n + x] = Cvt<T>::from(v[q] * scale);
+        for (int q = 0; q < Q; ++q) B[q * G.n + x] = Cvt<T>::from(v[q] * scale);
     }
 }
 
@@ -396,40 +398,41 @@ cudaError_t launch_objective(int Q, int storage, int lstorage, int mode, const O
 }
 
 cudaError_t launch_canon_pop(int Q, int storage, const Geometry& G, const void* pop, const uint32_t* mask,
-                             const PortMap* ports, int parity, int apply_ports, float* out, int grid,
-                             cudaStream_t s) {
+                             const PortMap* ports, int apply_ports, float* out, int grid, cudaStream_t s) {
     if (Q == 19) {
         LBM_STORAGE_DISPATCH(storage, T,
                              k_canon_pop<19, T><<<grid, BLOCK, 0, s>>>(G, static_cast<const T*>(pop), mask, ports,
-                                                                        parity, apply_ports, out))
+                                                                        apply_ports, out))
     } else {
         LBM_STORAGE_DISPATCH(storage, T,
                              k_canon_pop<27, T><<<grid, BLOCK, 0, s>>>(G, static_cast<const T*>(pop), mask, ports,
-                                                                        parity, apply_ports, out))
+                                                                        apply_ports, out))
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_upload_pop(int Q, int storage, const Geometry& G, void* pop, const float* in, int grid,
-                              cudaStream_t s) {
+cudaError_t launch_upload_pop(int Q, int storage, const Geometry& G, void* pop, const uint32_t* mask,
+                              const float* in, int grid, cudaStream_t s) {
     if (Q == 19) {
-        LBM_STORAGE_DISPATCH(storage, T, k_upload_pop<19, T><<<grid, BLOCK, 0, s>>>(G, static_cast<T*>(pop), in))
+        LBM_STORAGE_DISPATCH(storage, T,
+                             k_upload_pop<19, T><<<grid, BLOCK, 0, s>>>(G, static_cast<T*>(pop), mask, in))
     } else {
-        LBM_STORAGE_DISPATCH(storage, T, k_upload_pop<27, T><<<grid, BLOCK, 0, s>>>(G, static_cast<T*>(pop), in))
+        LBM_STORAGE_DISPATCH(storage, T,
+                             k_upload_pop<27, T><<<grid, BLOCK, 0, s>>>(G, static_cast<T*>(pop), mask, in))
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_canon_lam(int Q, int lstorage, const Geometry& G, const void* lam, const uint32_t* mask,
-                             int after_odd, float inv_scale, float* out, int grid, cudaStream_t s) {
+                             float inv_scale, float* out, int grid, cudaStream_t s) {
     if (Q == 19) {
         LBM_STORAGE_DISPATCH(lstorage, T,
                              k_canon_lam<19, T><<<grid, BLOCK, 0, s>>>(G, static_cast<const T*>(lam), mask,
-                                                                        after_odd, inv_scale, out))
+                                                                        inv_scale, out))
     } else {
         LBM_STORAGE_DISPATCH(lstorage, T,
                              k_canon_lam<27, T><<<grid, BLOCK, 0, s>>>(G, static_cast<const T*>(lam), mask,
-                                                                        after_odd, inv_scale, out))
+                                                                        inv_scale, out))
     }
     return cudaGetLastError();
 }

@@ -278,9 +278,8 @@ size_t storage_bytes(int s) { return s == LBM_STORE_F32 ? 4 : 2; }
 }  // namespace
 
 struct Checkpoint {
-    std::unique_ptr<DevBuf> buf;
+    std::unique_ptr<DevBuf> buf;  // the current population array (one of the two)
     int64_t t;
-    int parity;
     bool pending;
 };
 
@@ -311,15 +310,25 @@ struct lbm_handle {
     std::vector<StepDiag> last_trajectory;
     // --- state
     bool design_set = false, state_valid = false, forward_done = false;
-    int parity = 0;
+    int cur = 0;   // which population array holds the current state
+    int lcur = 0;  // which adjoint array holds the current adjoint state
     bool pending = false;
     int64_t t = 0;
     std::string err;
 
     int64_t n() const { return G.n; }
-    // population / adjoint planes start after the front padding
-    void* popA() const { return static_cast<char*>(pop.p) + pop_pad(G) * (storage == LBM_STORE_F32 ? 4 : 2); }
-    void* lamA() const { return static_cast<char*>(lam.p) + pop_pad(G) * (lam_storage == LBM_STORE_F32 ? 4 : 2); }
+    // One array (Q planes plus front and back padding) of the given storage.
+    size_t array_bytes(int st) const { return ((size_t)G.n * Q + 2 * pop_pad(G)) * (st == LBM_STORE_F32 ? 4 : 2); }
+    char* pop_array(int k) const { return static_cast<char*>(pop.p) + (size_t)k * array_bytes(storage); }
+    // planes start after the front padding: current (A) and other (B) array
+    void* popA() const { return pop_array(cur) + pop_pad(G) * (storage == LBM_STORE_F32 ? 4 : 2); }
+    void* popB() const { return pop_array(cur ^ 1) + pop_pad(G) * (storage == LBM_STORE_F32 ? 4 : 2); }
+    void* lam_plane0(int k) const {
+        return static_cast<char*>(lam.p) + (size_t)k * array_bytes(lam_storage) +
+               pop_pad(G) * (lam_storage == LBM_STORE_F32 ? 4 : 2);
+    }
+    void* lamA() const { return lam_plane0(lcur); }
+    void* lamB() const { return lam_plane0(lcur ^ 1); }
 };
 
 namespace {
@@ -429,7 +438,16 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
             for (int i = 0; i < h.Q; ++i) {
                 h.P.proj_left[j][i] = (float)(h.L.w[i] * rows[k][i] / norms[k]);
                 h.P.proj_right[j][i] = (float)rows[k][i];
+                h.P.proj_lw[j][i] = (float)(rows[k][i] / norms[k]);
             }
+            double m0 = 0, m2[6] = {0, 0, 0, 0, 0, 0};
+            const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+            for (int i = 0; i < h.Q; ++i) {
+                m0 += h.L.w[i] * rows[k][i];
+                for (int e = 0; e < 6; ++e) m2[e] += h.L.w[i] * rows[k][i] * h.L.c[i][ia[e]] * h.L.c[i][ib[e]];
+            }
+            h.P.proj_m0[j] = (float)m0;
+            for (int e = 0; e < 6; ++e) h.P.proj_m2[j][e] = (float)m2[e];
         }
     }
 
@@ -600,7 +618,7 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
     CK(cudaEventCreate(&h.ev0));
     CK(cudaEventCreate(&h.ev1));
     int64_t* ctr = &h.device_bytes;
-    h.pop.alloc(((size_t)n * h.Q + 2 * pop_pad(h.G)) * storage_bytes(h.storage), ctr);
+    h.pop.alloc(2 * h.array_bytes(h.storage), ctr);
     h.mask.alloc((size_t)(n + CELL_PAD) * 4, ctr);
     h.alpha.alloc((size_t)(n + CELL_PAD) * 4, ctr);
     h.errflag.alloc(sizeof(int), ctr);
@@ -645,7 +663,9 @@ FwdArgs fwd_args(lbm_handle& h) {
     FwdArgs a{};
     a.G = h.G;
     a.P = h.P;
-    a.pop = h.popA();
+    a.src = h.popA();
+    a.dst = h.popB();
+    a.bulk_store = h.G.n % (int64_t)(16 / storage_bytes(h.storage)) == 0 ? 1 : 0;
     a.mask = h.mask.as<uint32_t>();
     a.alpha = h.alpha.as<float>();
     a.ports = h.ports_d.as<PortMap>();
@@ -659,14 +679,13 @@ int coll_kind(const lbm_handle& h) { return h.coll == LBM_MRT ? CK_MRT : CK_PAIR
 // One step of the current state; diag / record optional.
 void step(lbm_handle& h, StepDiag* diag, float* record) {
     FwdArgs a = fwd_args(h);
-    a.parity = h.parity;
     a.apply_ports = h.pending ? 1 : 0;
     a.diag = diag;
     a.record = record;
     a.collide = 1;
     a.step = (uint32_t)h.t;
     CK(launch_forward(h.Q, coll_kind(h), h.storage, a, grid_for(h), h.stream));
-    h.parity ^= 1;
+    h.cur ^= 1;
     h.pending = h.n_ports > 0;
     ++h.t;
 }
@@ -674,7 +693,7 @@ void step(lbm_handle& h, StepDiag* diag, float* record) {
 // Load-only pass of the current state (admission reductions and/or record).
 void inspect(lbm_handle& h, StepDiag* diag, float* record) {
     FwdArgs a = fwd_args(h);
-    a.parity = h.parity;
+    a.dst = nullptr;
     a.apply_ports = h.pending ? 1 : 0;
     a.diag = diag;
     a.record = record;
@@ -683,8 +702,9 @@ void inspect(lbm_handle& h, StepDiag* diag, float* record) {
 }
 
 void init_state(lbm_handle& h) {
+    // both arrays: solid cells keep their populations in either
     CK(launch_init(h.Q, h.storage, h.G, h.P, h.popA(), h.mask.as<uint32_t>(), h.stream));
-    h.parity = 0;
+    CK(launch_init(h.Q, h.storage, h.G, h.P, h.popB(), h.mask.as<uint32_t>(), h.stream));
     h.pending = false;
     h.t = 0;
     h.state_valid = true;
@@ -773,10 +793,10 @@ lbm_status run_admitted(lbm_handle& h, int64_t steps, lbm_diag_t* out, int64_t K
             // checkpoint of the state entering step s (scan.rs:181-196)
             Checkpoint c;
             c.buf = std::make_unique<DevBuf>();
-            c.buf->alloc(h.pop.bytes, ctr);
-            CK(cudaMemcpyAsync(c.buf->p, h.pop.p, h.pop.bytes, cudaMemcpyDeviceToDevice, h.stream));
+            const size_t ab = h.array_bytes(h.storage);
+            c.buf->alloc(ab, ctr);
+            CK(cudaMemcpyAsync(c.buf->p, h.pop_array(h.cur), ab, cudaMemcpyDeviceToDevice, h.stream));
             c.t = h.t;
-            c.parity = h.parity;
             c.pending = h.pending;
             h.ckpts.push_back(std::move(c));
         }
@@ -805,7 +825,6 @@ ObjArgs obj_args(lbm_handle& h) {
     a.alpha = h.alpha.as<float>();
     a.phi = h.phi.as<float>();
     a.ports = h.ports_d.as<PortMap>();
-    a.parity = h.parity;
     a.apply_ports = h.pending ? 1 : 0;
     a.tau = (float)h.tau;
     a.vel = (float)(h.dx / h.dt);
@@ -879,7 +898,6 @@ void design_transpose(lbm_handle& h, const float* phibar, const float* abar, flo
 
 // ------------------------------------------------------------ adjoint
 struct AdjState {
-    int parity = 1;         // the first adjoint step after a seed gathers (parity 1)
     float scale = 1.f;      // stored = true * scale for the lambda now in memory
     float target = 1.f;     // scale the next adjoint step writes with
     float s0 = 1.f;         // abar is accumulated in units of 1/s0
@@ -891,7 +909,8 @@ AdjArgs adj_args(lbm_handle& h) {
     AdjArgs a{};
     a.G = h.G;
     a.P = h.P;
-    a.lam = h.lamA();
+    a.src = h.lamA();
+    a.dst = h.lamB();
     a.mask = h.mask.as<uint32_t>();
     a.alpha = h.alpha.as<float>();
     a.ports = h.ports_d.as<PortMap>();
@@ -906,7 +925,6 @@ AdjArgs adj_args(lbm_handle& h) {
 void adjoint_step(lbm_handle& h, AdjState& st, const float* rec, bool want_norm) {
     AdjArgs a = adj_args(h);
     a.record = rec;
-    a.parity = st.parity;
     a.port_transpose = 1;
     a.overwrite_abar = st.first ? 1 : 0;
     a.in_scale_inv = 1.f / st.scale;
@@ -914,7 +932,7 @@ void adjoint_step(lbm_handle& h, AdjState& st, const float* rec, bool want_norm)
     a.abar_factor = st.s0;
     a.norm2 = want_norm ? h.norm2.as<double>() : nullptr;
     CK(launch_adjoint(h.Q, coll_kind(h), h.lam_storage, a, grid_for(h), h.stream));
-    st.parity ^= 1;
+    h.lcur ^= 1;
     st.scale = st.target;
     st.first = false;
     ++st.steps;
@@ -965,7 +983,6 @@ double seed(lbm_handle& h, const double* w, AdjState& st, float* record) {
     a.norm2 = nullptr;
     a.record = nullptr;
     CK(launch_objective(h.Q, h.storage, h.lam_storage, 1, a, grid_for(h), h.stream));
-    st.parity = 1;
     st.first = true;
     return n0;
 }
@@ -975,7 +992,7 @@ void alloc_adjoint(lbm_handle& h, int lam_storage) {
     const int64_t n = h.n();
     if (h.lam.p && h.lam_storage != lam_storage) h.lam.reset();
     h.lam_storage = lam_storage;
-    h.lam.alloc(((size_t)n * h.Q + 2 * pop_pad(h.G)) * storage_bytes(lam_storage), ctr);
+    h.lam.alloc(2 * h.array_bytes(lam_storage), ctr);
     h.abar.alloc((size_t)n * 4, ctr);
     h.norm2.alloc(2 * sizeof(double), ctr);
 }
@@ -1103,8 +1120,7 @@ lbm_status gradient_horizon(lbm_handle& h, const double* w, const lbm_adjoint_op
         for (int64_t ci = (int64_t)h.ckpts.size() - 1; ci >= 0; --ci) {
             Checkpoint& c = h.ckpts[ci];
             const int64_t start = c.t, end = std::min(start + K, T);
-            CK(cudaMemcpyAsync(h.pop.p, c.buf->p, h.pop.bytes, cudaMemcpyDeviceToDevice, h.stream));
-            h.parity = c.parity;
+            CK(cudaMemcpyAsync(h.pop_array(h.cur), c.buf->p, c.buf->bytes, cudaMemcpyDeviceToDevice, h.stream));
             h.pending = c.pending;
             h.t = c.t;
             CK(cudaEventRecord(ef0, h.stream));
@@ -1329,9 +1345,11 @@ lbm_status lbm_set_populations(lbm_handle* h, const double* f, size_t n) {
         ensure_scratch(*h);
         CK(cudaMemcpyAsync(h->scratch.p, g.data(), g.size() * 4, cudaMemcpyHostToDevice, h->stream));
         const int grid = grid_for(*h);
-        CK(launch_upload_pop(Q, h->storage, h->G, h->popA(), h->scratch.as<float>(), grid, h->stream));
+        // both arrays: solid cells keep their populations in either
+        for (int k = 0; k < 2; ++k)
+            CK(launch_upload_pop(Q, h->storage, h->G, k ? h->popB() : h->popA(), h->mask.as<uint32_t>(),
+                                 h->scratch.as<float>(), grid, h->stream));
         CK(cudaStreamSynchronize(h->stream));
-        h->parity = 0;
         h->pending = false;
         h->t = 0;
         h->state_valid = true;
@@ -1348,7 +1366,7 @@ lbm_status lbm_get_populations(lbm_handle* h, double* f, size_t n) {
         check_n(*h, n, (size_t)(N * Q), "populations");
         ensure_scratch(*h);
         CK(launch_canon_pop(Q, h->storage, h->G, h->popA(), h->mask.as<uint32_t>(), h->ports_d.as<PortMap>(),
-                            h->parity, h->pending ? 1 : 0, h->scratch.as<float>(), grid_for(*h), h->stream));
+                            h->pending ? 1 : 0, h->scratch.as<float>(), grid_for(*h), h->stream));
         std::vector<float> g((size_t)N * Q);
         CK(cudaMemcpyAsync(g.data(), h->scratch.p, g.size() * 4, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
@@ -1457,16 +1475,15 @@ lbm_status lbm_step_vjp(lbm_handle* h, const double* state, const double* lambda
                            h->scratch.as<float>(), 1.f, 1, grid_for(*h), h->stream));
         AdjArgs a = adj_args(*h);
         a.record = h->record.as<float>();
-        a.lam = h->lamA();
-        a.parity = 1;
         a.port_transpose = 0;
         a.overwrite_abar = 1;
         a.in_scale_inv = 1.f;
         a.out_scale = 1.f;
         a.abar_factor = 1.f;
         CK(launch_adjoint(Q, coll_kind(*h), LBM_STORE_F32, a, grid_for(*h), h->stream));
+        h->lcur ^= 1;
         check_errflag(*h);
-        CK(launch_canon_lam(Q, LBM_STORE_F32, h->G, h->lamA(), h->mask.as<uint32_t>(), 1, 1.f, h->scratch.as<float>(),
+        CK(launch_canon_lam(Q, LBM_STORE_F32, h->G, h->lamA(), h->mask.as<uint32_t>(), 1.f, h->scratch.as<float>(),
                             grid_for(*h), h->stream));
         CK(cudaMemcpyAsync(v.data(), h->scratch.p, v.size() * 4, cudaMemcpyDeviceToHost, h->stream));
         std::vector<float> ab((size_t)N);
