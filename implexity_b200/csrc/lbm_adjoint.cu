@@ -26,9 +26,10 @@ struct AdjStage {
 template <int Q, int COLL, typename T>
 __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
     using S = AdjStage<Q, T>;
+    constexpr int NCOPY = Q + 6;  // runs of lambda, the record, mask and alpha
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem);
-    uint64_t* empty = full + STAGES;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem);  // stage loaded
+    uint64_t* empty = full + STAGES;                      // stage consumed
     const T* B = static_cast<const T*>(a.src);
     T* D = static_cast<T*>(a.dst);
     const uint32_t n = (uint32_t)a.G.n;
@@ -45,71 +46,74 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
     }
     __syncthreads();
     if (warp == 0) {
-        if (lane == 0) {
-            int s = 0;
-            uint32_t round = 0;
-            for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-                if (round > 0 && !mbar_wait(&empty[s], (round - 1) & 1u, a.err)) break;
-                S* st = stage_at<S>(smem, s);
-                const uint32_t x0 = tile * TILE;
-                mbar_expect_tx(&full[s], Q * Vec16<T>::BYTES + 6 * FRUN_BYTES);
+        // producer warp, as in the forward step: each lane issues its runs' copies.
+        // (The outputs leave through direct stores: this step is bound by its
+        // arithmetic, and staging the outputs would add a block-wide wait.)
+        const uint32_t mine = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 #pragma unroll 1
-                for (int q = 0; q < Q; ++q) bulk_g2s(&st->run[q][0], B + (a.run0[q] + x0), Vec16<T>::BYTES, &full[s]);
+        for (uint32_t i = 0; i < mine + STAGES; ++i) {
+            const int s = (int)(i % STAGES);
+            const uint32_t round = i / STAGES;
+            S* st = stage_at<S>(smem, s);
+            if (round > 0) {
+                bool done = true;
+                if (lane == 0) done = mbar_wait(&empty[s], (round - 1) & 1u, a.err);
+                if (!__shfl_sync(0xffffffffu, done, 0)) break;
+            }
+            if (i < mine) {
+                const uint32_t x0 = (blockIdx.x + i * gridDim.x) * TILE;
+                if (lane == 0) mbar_expect_tx(&full[s], Q * Vec16<T>::BYTES + 6 * FRUN_BYTES);
+                __syncwarp();
 #pragma unroll 1
-                for (int k = 0; k < 4; ++k) bulk_g2s(&st->rec[k][0], a.record + (a.rec0[k] + x0), FRUN_BYTES, &full[s]);
-                bulk_g2s(&st->mask[0], a.mask + x0, FRUN_BYTES, &full[s]);
-                bulk_g2s(&st->alpha[0], a.alpha + x0, FRUN_BYTES, &full[s]);
-                if (++s == STAGES) {
-                    s = 0;
-                    ++round;
+                for (int k = lane; k < NCOPY; k += 32) {
+                    if (k < Q) bulk_g2s(&st->run[k][0], B + (a.run0[k] + x0), Vec16<T>::BYTES, &full[s]);
+                    else if (k < Q + 4)
+                        bulk_g2s(&st->rec[k - Q][0], a.record + (a.rec0[k - Q] + x0), FRUN_BYTES, &full[s]);
+                    else if (k == Q + 4) bulk_g2s(&st->mask[0], a.mask + x0, FRUN_BYTES, &full[s]);
+                    else bulk_g2s(&st->alpha[0], a.alpha + x0, FRUN_BYTES, &full[s]);
                 }
             }
         }
     } else {
-        const int c0 = threadIdx.x - 32;
+        const int c = threadIdx.x - 32;
         int s = 0;
         uint32_t round = 0;
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
             const bool ok = mbar_wait(&full[s], round & 1u, a.err);
             const S* st = stage_at<S>(smem, s);
-#pragma unroll 1
-            for (int k = 0; k < CPT; ++k) {
-                const int c = c0 + k * (CONSUMER_WARPS * 32);
-                const uint32_t x = tile * TILE + c;
-                if (ok && x < n) {
-                    const uint32_t m = st->mask[c];
-                    if (!(m & MASK_SOLID)) {
-                        float v[Q];
-                        if (!(m & MASK_WRAP)) {
+            const uint32_t x = tile * TILE + c;
+            const uint32_t m = ok && x < n ? st->mask[c] : MASK_SOLID;
+            const bool fluid = !(m & MASK_SOLID);
+            float v[Q];
+            if (fluid) {
+                if (!(m & MASK_WRAP)) {
 #pragma unroll
-                            for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(st->run[q][a.rund[q] + c]);
-                            if (m & LINK_BITS) {
-                                // transposed bounce-back: the cell's own opposite slot
+                    for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(st->run[q][a.rund[q] + c]);
+                    if (m & LINK_BITS) {
+                        // transposed bounce-back: the cell's own opposite slot
 #pragma unroll
-                                for (int q = 1; q < Q; ++q)
-                                    if ((m >> opp<Q>(q)) & 1u) v[q] = Cvt<T>::to(B[opp<Q>(q) * n + x]);
-                            }
+                        for (int q = 1; q < Q; ++q)
+                            if ((m >> opp<Q>(q)) & 1u) v[q] = Cvt<T>::to(B[opp<Q>(q) * n + x]);
+                    }
 #pragma unroll
-                            for (int q = 0; q < Q; ++q) v[q] *= a.in_scale_inv;
-                        } else {
+                    for (int q = 0; q < Q; ++q) v[q] *= a.in_scale_inv;
+                } else {
 #pragma unroll
-                            for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(B[pull_adj_index<Q>(a.G, x, m, q)]) * a.in_scale_inv;
-                        }
-                        const float u[3] = {st->rec[1][a.recd[1] + c], st->rec[2][a.recd[2] + c],
-                                            st->rec[3][a.recd[3] + c]};
-                        const float ab = collide_vjp<Q, COLL>(v, st->rec[0][a.recd[0] + c], u, st->alpha[c], a.P);
-                        if (a.overwrite_abar) a.abar[x] = ab * a.abar_factor;
-                        else a.abar[x] = fmaf(ab, a.abar_factor, a.abar[x]);
-                        if (a.port_transpose && (m & MASK_PORT))
-                            port_transpose<Q>(a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], v);
-                        store_own_lam<Q, T>(D, n, x, v, a.out_scale);
-                        if (a.norm2) {
+                    for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(B[pull_adj_index<Q>(a.G, x, m, q)]) * a.in_scale_inv;
+                }
+            }
+            if (fluid) {
+                const float u[3] = {st->rec[1][a.recd[1] + c], st->rec[2][a.recd[2] + c], st->rec[3][a.recd[3] + c]};
+                const float ab = collide_vjp<Q, COLL>(v, st->rec[0][a.recd[0] + c], u, st->alpha[c], a.P);
+                if (a.overwrite_abar) a.abar[x] = ab * a.abar_factor;
+                else a.abar[x] = fmaf(ab, a.abar_factor, a.abar[x]);
+                if (a.port_transpose && (m & MASK_PORT)) port_transpose<Q>(a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], v);
+                store_own_lam<Q, T>(D, n, x, v, a.out_scale);
+                if (a.norm2) {
 #pragma unroll
-                            for (int q = 0; q < Q; ++q) {
-                                const float sv = v[q] * a.out_scale;
-                                nsum += (double)sv * (double)sv;
-                            }
-                        }
+                    for (int q = 0; q < Q; ++q) {
+                        const float sv = v[q] * a.out_scale;
+                        nsum += (double)sv * (double)sv;
                     }
                 }
             }

@@ -830,8 +830,7 @@ namespace {
 // run's misalignment.  Blocked links (walls, solids) and cells on periodic
 // faces read their few populations from global memory directly.
 constexpr int CONSUMER_WARPS = 8;
-constexpr int CPT = 1;                         // cells per consumer thread and tile
-constexpr int TILE = CONSUMER_WARPS * 32 * CPT;
+constexpr int TILE = CONSUMER_WARPS * 32;
 constexpr int TPB = CONSUMER_WARPS * 32 + 32;
 constexpr int STAGES = 3;
 
