@@ -23,7 +23,7 @@ struct AdjStage {
     float alpha[FRUN];
 };
 
-template <int Q, int COLL, typename T>
+template <int Q, int COLL, typename T, int AL>
 __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
     using S = AdjStage<Q, T>;
     constexpr int NCOPY = Q + 6;  // runs of lambda, the record, mask and alpha
@@ -88,7 +88,8 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
             if (fluid) {
                 if (!(m & MASK_WRAP)) {
 #pragma unroll
-                    for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(st->run[q][a.rund[q] + c]);
+                    for (int q = 0; q < Q; ++q)
+                        v[q] = Cvt<T>::to(st->run[q][(AL ? rund_aligned<Q, T, 1>(q) : a.rund[q]) + c]);
                     if (m & LINK_BITS) {
                         // transposed bounce-back: the cell's own opposite slot
 #pragma unroll
@@ -133,18 +134,32 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
     }
 }
 
-template <int Q, int COLL, typename T>
-cudaError_t run_adjoint(const AdjArgs& a, cudaStream_t s) {
+template <int Q, int COLL, typename T, int AL>
+cudaError_t run_adjoint_al(const AdjArgs& a, cudaStream_t s) {
     constexpr size_t smem = pipe_bytes<AdjStage<Q, T>>();
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = set_smem(k_adjoint<Q, COLL, T>, smem);
+        cudaError_t e = set_smem(k_adjoint<Q, COLL, T, AL>, smem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    const int grid = persistent_grid((const void*)k_adjoint<Q, COLL, T>, a.G.n, smem, TPB, TILE);
-    k_adjoint<Q, COLL, T><<<grid, TPB, smem, s>>>(a);
+    const int grid = persistent_grid((const void*)k_adjoint<Q, COLL, T, AL>, a.G.n, smem, TPB, TILE);
+    k_adjoint<Q, COLL, T, AL><<<grid, TPB, smem, s>>>(a);
     return cudaGetLastError();
+}
+
+template <int Q, typename T>
+bool adj_table_is_aligned(const int32_t* rund) {
+    for (int q = 0; q < Q; ++q) {
+        const int d = Q == 19 ? Lat<19>::cz(q) : Lat<27>::cz(q);
+        if (rund[q] != (d < 0 ? d + Vec16<T>::V : d)) return false;
+    }
+    return true;
+}
+
+template <int Q, int COLL, typename T>
+cudaError_t run_adjoint(const AdjArgs& a, cudaStream_t s) {
+    return adj_table_is_aligned<Q, T>(a.rund) ? run_adjoint_al<Q, COLL, T, 1>(a, s) : run_adjoint_al<Q, COLL, T, 0>(a, s);
 }
 
 }  // namespace
@@ -158,6 +173,10 @@ cudaError_t launch_adjoint(int Q, int coll, int lstorage, const AdjArgs& a0, int
         a.recd[k] = (int32_t)(first % 4);
         a.rec0[k] = first - a.recd[k];
     }
+    // every bulk copy needs 16-byte aligned addresses: refuse to launch otherwise
+    if (!staged_aligned(a.src, a.run0, Q, lstorage == ST_F32 ? 4 : 2) || !staged_aligned(a.record, a.rec0, 4, 4) ||
+        !staged_aligned(a.mask, nullptr, 0, 4) || !staged_aligned(a.alpha, nullptr, 0, 4))
+        return cudaErrorMisalignedAddress;
     if (Q == 19) {
         if (coll == CK_MRT) {
             LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint<19, CK_MRT, T>(a, s))

@@ -856,6 +856,39 @@ __device__ __forceinline__ S* stage_at(unsigned char* smem, int s) {
     return reinterpret_cast<S*>(smem + 128 + s * stage_stride<S>());
 }
 
+// Misalignment of direction q's staged run when the plane stride n and the
+// strides sx, sy are multiples of the 16-byte vector V: the run starts at
+// q*n + x0 + dir*lin(q) and x0 is a multiple of the tile, so only c_z is left.
+template <int Q, typename T, int DIR>
+__device__ __forceinline__ constexpr int rund_aligned(int q) {
+    constexpr int V = Vec16<T>::V;
+    const int d = DIR * Lat<Q>::cz(q);
+    return d < 0 ? d + V : d;
+}
+
+// Minimum population f = w + g (or w (1 + g/w) in 16-bit storage units) of
+// one cell: the minimum is taken per weight class (|c|^2) first.
+template <int Q, int SC>
+__device__ __forceinline__ float min_population(const float (&v)[Q]) {
+    using L = Lat<Q>;
+    float m[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int k = (L::cx(q) != 0) + (L::cy(q) != 0) + (L::cz(q) != 0);
+        m[k] = fminf(m[k], v[q]);
+    }
+    float mn = INFINITY;
+#pragma unroll
+    for (int k = 0; k < (Q == 19 ? 3 : 4); ++k) {
+        float w = 0.f;  // the class weight (a compile-time constant after unrolling)
+#pragma unroll
+        for (int r = 0; r < Q; ++r)
+            if ((L::cx(r) != 0) + (L::cy(r) != 0) + (L::cz(r) != 0) == k) w = L::w(r);
+        mn = fminf(mn, SC ? w * (1.f + m[k]) : w + m[k]);
+    }
+    return mn;
+}
+
 // Aligned store of one cell's values into its own slots of the output array
 // (populations in storage units with stochastic rounding for 16-bit storage,
 // or adjoint values scaled by `scale`).

@@ -22,7 +22,7 @@ struct FwdStage {
     float alpha[FRUN];
 };
 
-template <int Q, int COLL, typename T>
+template <int Q, int COLL, typename T, int AL>
 __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
     using L = Lat<Q>;
     using S = FwdStage<Q, T>;
@@ -106,7 +106,8 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
             if (fluid) {
                 if (!(m & MASK_WRAP)) {
 #pragma unroll
-                    for (int q = 0; q < Q; ++q) v[q] = sdec<T>(st->run[q][a.rund[q] + c]);
+                    for (int q = 0; q < Q; ++q)
+                        v[q] = sdec<T>(st->run[q][(AL ? rund_aligned<Q, T, -1>(q) : a.rund[q]) + c]);
                     if (m & LINK_BITS) {
                         // halfway bounce-back: the cell's own opposite slot
 #pragma unroll
@@ -135,11 +136,7 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
                         for (int q = 0; q < Q; ++q) v[q] *= (float)(1.0 / L::wd(q));
                     }
                 }
-                float mn = INFINITY;
-                if (a.diag) {
-#pragma unroll
-                    for (int q = 0; q < Q; ++q) mn = fminf(mn, SC ? L::w(q) * (1.f + v[q]) : L::w(q) + v[q]);
-                }
+                const float mn = a.diag ? min_population<Q, SC>(v) : 0.f;
                 const Macro M = collide_fused<Q, COLL, SC>(v, alpha, a.P, a.collide);
                 if (a.diag) {
                     acc.mass += M.rp;
@@ -184,21 +181,45 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
     if (a.diag) finish_diag(acc, a.diag, a.red);
 }
 
-template <int Q, int COLL, typename T>
-cudaError_t run_forward(const FwdArgs& a, cudaStream_t s) {
+template <int Q, int COLL, typename T, int AL>
+cudaError_t run_forward_al(const FwdArgs& a, cudaStream_t s) {
     constexpr size_t smem = pipe_bytes<FwdStage<Q, T>>();
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = set_smem(k_forward<Q, COLL, T>, smem);
+        cudaError_t e = set_smem(k_forward<Q, COLL, T, AL>, smem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    const int grid = persistent_grid((const void*)k_forward<Q, COLL, T>, a.G.n, smem, TPB, TILE);
-    k_forward<Q, COLL, T><<<grid, TPB, smem, s>>>(a);
+    const int grid = persistent_grid((const void*)k_forward<Q, COLL, T, AL>, a.G.n, smem, TPB, TILE);
+    k_forward<Q, COLL, T, AL><<<grid, TPB, smem, s>>>(a);
     return cudaGetLastError();
 }
 
+// The run offsets are compile-time constants when every run table entry
+// matches rund_aligned (plane stride and strides multiples of the vector).
+template <int Q, typename T, int DIR>
+bool table_is_aligned(const int32_t* rund) {
+    for (int q = 0; q < Q; ++q) {
+        const int d = DIR * (Q == 19 ? Lat<19>::cz(q) : Lat<27>::cz(q));
+        if (rund[q] != (d < 0 ? d + Vec16<T>::V : d)) return false;
+    }
+    return true;
+}
+
+template <int Q, int COLL, typename T>
+cudaError_t run_forward(const FwdArgs& a, cudaStream_t s) {
+    return table_is_aligned<Q, T, -1>(a.rund) ? run_forward_al<Q, COLL, T, 1>(a, s) : run_forward_al<Q, COLL, T, 0>(a, s);
+}
+
 }  // namespace
+
+bool staged_aligned(const void* base, const int64_t* run0, int nrun, size_t elem) {
+    const uintptr_t b = reinterpret_cast<uintptr_t>(base);
+    if (b % 16) return false;
+    for (int q = 0; q < nrun; ++q)
+        if ((b + (uintptr_t)(run0[q] * (int64_t)elem)) % 16) return false;
+    return true;
+}
 
 void run_table(int Q, const Geometry& G, int dir, int vec, int64_t* run0, int32_t* rund) {
     for (int q = 0; q < Q; ++q) {
@@ -217,6 +238,11 @@ cudaError_t launch_forward(int Q, int coll, int storage, const FwdArgs& a0, int 
     (void)grid;
     FwdArgs a = a0;
     run_table(Q, a.G, -1, storage == ST_F32 ? 4 : 8, a.run0, a.rund);
+    // every bulk copy needs 16-byte aligned addresses: refuse to launch otherwise
+    const size_t es = storage == ST_F32 ? 4 : 2;
+    if (!staged_aligned(a.src, a.run0, Q, es) || !staged_aligned(a.mask, nullptr, 0, 4) ||
+        !staged_aligned(a.alpha, nullptr, 0, 4) || (a.bulk_store && !staged_aligned(a.dst, nullptr, 0, es)))
+        return cudaErrorMisalignedAddress;
     if (Q == 19) {
         if (coll == CK_MRT) {
             LBM_STORAGE_DISPATCH(storage, T, return run_forward<19, CK_MRT, T>(a, s))

@@ -120,6 +120,8 @@ struct DesignArgs {
 // first used element q*n + x0 + dir*lin(q) (dir -1: forward pull, +1:
 // adjoint pull), aligned down to `vec` elements.
 void run_table(int Q, const Geometry& G, int dir, int vec, int64_t* run0, int32_t* rund);
+// True when base and every run start base + run0[q]*elem are 16-byte aligned.
+bool staged_aligned(const void* base, const int64_t* run0, int nrun, size_t elem);
 
 // Sets the message lbm_last_error(NULL) returns on this thread (entry points
 // that take no handle report through it).

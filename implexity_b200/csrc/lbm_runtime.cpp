@@ -317,8 +317,13 @@ struct lbm_handle {
     std::string err;
 
     int64_t n() const { return G.n; }
-    // One array (Q planes plus front and back padding) of the given storage.
-    size_t array_bytes(int st) const { return ((size_t)G.n * Q + 2 * pop_pad(G)) * (st == LBM_STORE_F32 ? 4 : 2); }
+    // One array (Q planes plus front and back padding) of the given storage,
+    // rounded up so that the second array starts 256-byte aligned like the
+    // first (the staged bulk copies need 16-byte aligned runs in both).
+    size_t array_bytes(int st) const {
+        const size_t b = ((size_t)G.n * Q + 2 * pop_pad(G)) * (st == LBM_STORE_F32 ? 4 : 2);
+        return (b + 255) / 256 * 256;
+    }
     char* pop_array(int k) const { return static_cast<char*>(pop.p) + (size_t)k * array_bytes(storage); }
     // planes start after the front padding: current (A) and other (B) array
     void* popA() const { return pop_array(cur) + pop_pad(G) * (storage == LBM_STORE_F32 ? 4 : 2); }
