@@ -31,15 +31,11 @@ from pathlib import Path
 
 import numpy as np
 
+from implexity_b200.workloads import CONFIGS
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-CONFIGS = {
-    # name: (shape, steps, collision, mrt_bulk, design)
-    "channel128_trt": ((128, 128, 128), 5000, "trt", None, "uniform"),
-    "channel256x128x128_mrt": ((256, 128, 128), 3000, "mrt", 1.2, "spheres"),
-    "channel48x24x24_trt": ((48, 24, 24), 2000, "trt", None, "uniform"),
-}
 FWD_BYTES = {  # algorithmic bytes per cell update: 2 Q s_f + 4 (alpha)
     ("float32", 19): 2 * 19 * 4 + 4,
     ("float16", 19): 2 * 19 * 2 + 4,

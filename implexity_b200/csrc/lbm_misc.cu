@@ -55,8 +55,78 @@ __global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
         float g[Q];
         load_pop<Q, T>(A, a.G, x, m, g);
         const PortMap* pm = (m & MASK_PORT) ? &a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1] : nullptr;
-        if (a.apply_ports && pm) apply_port<Q>(*pm, g);
         const float alpha = a.alpha[x];
+        if constexpr (MODE == 0) {
+            // Responses in FP64 from the stored populations: the viscous
+            // stress is a small difference of second moments, which FP32
+            // arithmetic would resolve to only ~1e-4 per cell.
+            double gd[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) gd[q] = g[q];
+            if (a.apply_ports && pm) {
+                double in[Q];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) in[q] = gd[q];
+#pragma unroll
+                for (int r = 0; r < Q; ++r) {
+                    if (pm->unknown_mask & (1u << r)) {
+                        double acc_r = pm->bias[r];
+#pragma unroll
+                        for (int kk = 0; kk < Q; ++kk) acc_r = fma((double)pm->jac[r][kk], in[kk], acc_r);
+                        gd[r] = acc_r;
+                    }
+                }
+            }
+            double rp = 0.0, j[3] = {0.0, 0.0, 0.0}, S2[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const int c0 = L::cx(q), c1 = L::cy(q), c2 = L::cz(q);
+                rp += gd[q];
+                if (c0) { j[0] += c0 * gd[q]; S2[0] += gd[q]; }
+                if (c1) { j[1] += c1 * gd[q]; S2[1] += gd[q]; }
+                if (c2) { j[2] += c2 * gd[q]; S2[2] += gd[q]; }
+                if (c0 && c1) S2[3] += c0 * c1 * gd[q];
+                if (c0 && c2) S2[4] += c0 * c2 * gd[q];
+                if (c1 && c2) S2[5] += c1 * c2 * gd[q];
+            }
+            const double rho = 1.0 + rp, sd = 1.0 + 0.5 * (double)alpha;
+            double ud[3], Fd[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                ud[d] = (j[d] / rho + 0.5 * (double)a.P.a[d]) / sd;
+                Fd[d] = rho * ((double)a.P.a[d] - (double)alpha * ud[d]);
+            }
+            const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+            const double kd = 1.0 - 0.5 / (double)a.tau, nud = ((double)a.tau - 0.5) / 3.0;
+            double ss = 0.0;
+#pragma unroll
+            for (int e = 0; e < 6; ++e) {
+                const double pi = S2[e] - (e < 3 ? rp / 3.0 : 0.0) - rho * ud[ia[e]] * ud[ib[e]];
+                const double t = 0.5 * (ud[ia[e]] * Fd[ib[e]] + ud[ib[e]] * Fd[ia[e]]);
+                const double sg = -kd * (pi + t);
+                ss += (e < 3 ? 1.0 : 2.0) * sg * sg;
+            }
+            const double V = a.vel;
+            const double U[3] = {ud[0] * V, ud[1] * V, ud[2] * V};
+            const double R = rho * a.dens;
+            const double usq = U[0] * U[0] + U[1] * U[1] + U[2] * U[2];
+            acc.add(0, U[0]);
+            acc.add(1, U[1]);
+            acc.add(2, U[2]);
+            acc.add(3, R * usq);
+            acc.add(4, R * (double)alpha / a.dt_s * usq);
+            acc.add(5, (double)a.phi[x]);
+            if (pm) acc.add(6, (double)pm->dp_weight * a.dens * rp * V * V / 3.0);
+            acc.add(7, ss / (2.0 * rho * nud));
+            if (a.fields) {
+                a.fields[x] = (float)rp;
+                a.fields[n + x] = (float)ud[0];
+                a.fields[2 * n + x] = (float)ud[1];
+                a.fields[3 * n + x] = (float)ud[2];
+            }
+            continue;
+        }
+        if (a.apply_ports && pm) apply_port<Q>(*pm, g);
         Macro M = macroscopic<Q>(g, alpha, a.P);
         // second moments of g: M2_ab = sum c_a c_b g (f adds delta/3)
         float S[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -83,25 +153,7 @@ __global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
             ss += (e < 3 ? 1.f : 2.f) * sig[e] * sig[e];
         }
         const float dpw = pm ? pm->dp_weight : 0.f;
-        if constexpr (MODE == 0) {
-            const float U[3] = {u[0] * a.vel, u[1] * a.vel, u[2] * a.vel};
-            const double R = (double)M.rho * a.dens;
-            const double usq = (double)U[0] * U[0] + (double)U[1] * U[1] + (double)U[2] * U[2];
-            acc.add(0, U[0]);
-            acc.add(1, U[1]);
-            acc.add(2, U[2]);
-            acc.add(3, R * usq);
-            acc.add(4, R * alpha / a.dt_s * usq);
-            acc.add(5, (double)a.phi[x]);
-            if (pm) acc.add(6, (double)dpw * a.dens * (double)M.rp * a.vel * a.vel / 3.0);
-            acc.add(7, (double)ss / (2.0 * M.rho * nu));
-            if (a.fields) {
-                a.fields[x] = M.rp;
-                a.fields[n + x] = u[0];
-                a.fields[2 * n + x] = u[1];
-                a.fields[3 * n + x] = u[2];
-            }
-        } else {
+        {
             // cotangents of rho, u, F, M2 (all lattice units)
             const float V = a.vel;
             const float U[3] = {u[0] * V, u[1] * V, u[2] * V};

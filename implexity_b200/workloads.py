@@ -17,6 +17,17 @@ NU = 1e-6
 DX = 1e-3
 
 
+# The seeded channel workloads: name -> (shape, forward steps, collision,
+# MRT bulk rate, design kind).
+CONFIGS = {
+    "channel128_trt": ((128, 128, 128), 5000, "trt", None, "uniform"),
+    "channel256x128x128_trt": ((256, 128, 128), 3000, "trt", None, "uniform"),
+    "channel256x128x128_mrt": ((256, 128, 128), 3000, "mrt", 1.2, "spheres"),
+    "channel48x24x24_trt": ((48, 24, 24), 2000, "trt", None, "uniform"),
+    "channel64_trt": ((64, 64, 64), 5000, "trt", None, "uniform"),
+}
+
+
 def channel_problem(
     shape=(48, 24, 24),
     steps=2000,

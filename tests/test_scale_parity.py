@@ -1,0 +1,61 @@
+"""FP32 GPU results against the FP64 oracle on the 64^3 channel (5000 steps,
+steady adjoint): velocity and density within 1e-5 relative, the objective
+within 1e-6, the steady gradient within 1e-4 relative L2 (FP16 storage:
+1e-3).  The oracle takes minutes at this size, so the test runs only with
+IMPLEXITY_SCALE_TESTS=1.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from implexity_b200 import LbmSolver, normalize, workloads
+from oracle.oracle import Oracle
+from test_gpu_parity import macroscopic, rel_max
+
+pytestmark = [
+    pytest.mark.gpu,
+    pytest.mark.skipif(os.environ.get("IMPLEXITY_SCALE_TESTS") != "1", reason="set IMPLEXITY_SCALE_TESTS=1"),
+]
+
+
+def _rel_l2(a, b):
+    a, b = np.ravel(a), np.ravel(b)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_channel64_against_fp64_oracle(gpu_lib):
+    shape, steps, coll, _, _ = workloads.CONFIGS["channel64_trt"]
+    w = workloads.objective_weights()
+    raw = workloads.uniform_design(shape, 0)
+    prob = workloads.channel_problem(shape=shape, steps=steps, collision=coll)
+    norm = normalize(prob)
+    o = Oracle(norm)
+    g_ref, r_ref, _, st = o.gradient(raw, w, mode="steady", tol=1e-12)
+    assert st == 0
+    phi_ref, alpha_ref = o.design(raw)
+    f_ref, _ = o.history(alpha_ref, steps)
+    report = {}
+    for storage in ("float32", "float16"):
+        p = workloads.channel_problem(shape=shape, steps=steps, collision=coll, storage=storage)
+        with LbmSolver(p) as s:
+            s.set_design(raw)
+            s.forward()
+            f = s.populations()
+            r = s.responses()
+            g, rep = s.gradient(w, mode="steady", tolerance=1e-8, lambda_storage=storage)
+        rho, u = macroscopic(f, s.q, alpha_ref, o.acceleration_lattice)
+        rho_r, u_r = macroscopic(f_ref, s.q, alpha_ref, o.acceleration_lattice)
+        report[storage] = {
+            "u_rel_max": rel_max(u, u_r),
+            "rho_max_abs": float(np.max(np.abs(rho - rho_r))),
+            "objective_rel": abs(np.dot(w, r) - np.dot(w, r_ref)) / abs(np.dot(w, r_ref)),
+            "grad_rel_l2": _rel_l2(g, g_ref),
+            "iterations": rep.iterations,
+        }
+    print(report)
+    assert report["float32"]["u_rel_max"] < 1e-5
+    assert report["float32"]["rho_max_abs"] < 1e-5
+    assert report["float32"]["objective_rel"] < 1e-6
+    assert report["float32"]["grad_rel_l2"] < 1e-4
+    assert report["float16"]["grad_rel_l2"] < 1e-3
