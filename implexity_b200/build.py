@@ -18,6 +18,8 @@ CSRC = PKG / "csrc"
 INCLUDE = PKG.parent / "include"
 BUILD = PKG / "_build"
 LIB = PKG / "liblbm_b200.so"
+MMA_LIB = PKG / "libmma_cpu.so"
+MMA_SOURCE = CSRC / "mma_cpu.cpp"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
@@ -44,7 +46,31 @@ def up_to_date() -> bool:
     return all(f.stat().st_mtime <= t for f in _inputs())
 
 
+def host_cxx() -> str:
+    """A host C++ compiler with OpenMP (the distribution g++ first)."""
+    for cand in (os.environ.get("MMA_CXX"), "/usr/bin/g++", shutil.which("g++")):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("g++ not found: a host C++ compiler with OpenMP is required to build libmma_cpu.so")
+
+
+def build_mma(force: bool = False, verbose: bool = False) -> Path:
+    """The host MMA library (include/mma_cpu.h): C++17 with OpenMP."""
+    deps = [MMA_SOURCE, INCLUDE / "mma_cpu.h"]
+    if not force and MMA_LIB.exists() and all(d.stat().st_mtime <= MMA_LIB.stat().st_mtime for d in deps):
+        return MMA_LIB
+    tmp = MMA_LIB.with_suffix(".so.tmp")
+    cmd = [host_cxx(), "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-fvisibility=hidden", "-Wall",
+           "-o", str(tmp), str(MMA_SOURCE)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, MMA_LIB)
+    return MMA_LIB
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
+    build_mma(force, verbose)
     if not force and up_to_date():
         return LIB
     BUILD.mkdir(exist_ok=True)
