@@ -9,7 +9,7 @@ import ctypes as C
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "liblbm_b200.so"
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # status codes
 LBM_OK, LBM_E_CONTRACT, LBM_E_CONVERGENCE, LBM_E_CUDA, LBM_E_STATE = 0, 1, 2, 3, 4
@@ -21,6 +21,7 @@ LBM_PORT_VELOCITY, LBM_PORT_PRESSURE = 0, 1
 FACES = ["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"]
 LBM_FILTER_CONIC, LBM_FILTER_BOX = 0, 1
 LBM_ADJ_HORIZON, LBM_ADJ_STEADY = 0, 1
+LBM_OBJ_FINAL, LBM_OBJ_TIME_AVERAGE = 0, 1
 N_RESPONSES = 8
 MAX_PORTS = 7
 
@@ -38,6 +39,7 @@ EXPORTS = [
     "lbm_advance",
     "lbm_trajectory",
     "lbm_responses",
+    "lbm_time_average",
     "lbm_fields",
     "lbm_gradient",
     "lbm_step_vjp",
@@ -53,6 +55,11 @@ class Port(C.Structure):
         ("mask", C.POINTER(C.c_uint8)),
         ("velocity_m_s", C.c_double * 3),
         ("gauge_pressure_Pa", C.c_double),
+        ("amplitude_m_s", C.c_double * 3),
+        ("amplitude_Pa", C.c_double),
+        ("frequency_hz", C.c_double),
+        ("phase_rad", C.c_double),
+        ("ramp_s", C.c_double),
     ]
 
 
@@ -86,6 +93,7 @@ class Problem(C.Structure):
         ("design_region", C.POINTER(C.c_uint8)),
         ("fixed_design", C.POINTER(C.c_double)),
         ("ports", C.POINTER(Port)),
+        ("time_average", C.c_int32),
     ]
 
 
@@ -112,6 +120,7 @@ class AdjointOpts(C.Structure):
         ("check_every", C.c_int64),
         ("tolerance", C.c_double),
         ("record_budget_bytes", C.c_int64),
+        ("objective", C.c_int32),
     ]
 
 
@@ -161,6 +170,7 @@ def _declare(lib: C.CDLL) -> None:
     lib.lbm_advance.argtypes = [h, C.c_int64, C.POINTER(Diag)]
     lib.lbm_trajectory.argtypes = [h, _dp, _dp, _dp, _dp, C.c_size_t]
     lib.lbm_responses.argtypes = [h, _dp]
+    lib.lbm_time_average.argtypes = [h, _dp]
     lib.lbm_fields.argtypes = [h, _dp, _dp, _dp]
     lib.lbm_gradient.argtypes = [h, _dp, C.POINTER(AdjointOpts), _dp, C.POINTER(AdjointReport)]
     lib.lbm_step_vjp.argtypes = [h, _dp, _dp, _dp, _dp, C.c_size_t]

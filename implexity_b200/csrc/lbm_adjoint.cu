@@ -15,18 +15,21 @@
 namespace lbm {
 namespace {
 
-template <int Q, typename T>
+template <int Q, typename T, int NREC>
 struct AdjStage {
     T run[Q][Vec16<T>::RUN];
-    float rec[4][FRUN];
+    float rec[NREC][FRUN];
     uint32_t mask[FRUN];
     float alpha[FRUN];
 };
 
-template <int Q, int COLL, typename T, int AL>
+// STG = 1: the stage-objective variant, which reads the second moments of
+// the recorded state as well and adds the state's response VJP.
+template <int Q, int COLL, typename T, int AL, int STG>
 __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
-    using S = AdjStage<Q, T>;
-    constexpr int NCOPY = Q + 6;  // runs of lambda, the record, mask and alpha
+    constexpr int NREC = STG ? 10 : 4;
+    using S = AdjStage<Q, T, NREC>;
+    constexpr int NCOPY = Q + NREC + 2;  // runs of lambda, the record, mask and alpha
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);  // stage loaded
     uint64_t* empty = full + STAGES;                      // stage consumed
@@ -62,14 +65,14 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
             }
             if (i < mine) {
                 const uint32_t x0 = (blockIdx.x + i * gridDim.x) * TILE;
-                if (lane == 0) mbar_expect_tx(&full[s], Q * Vec16<T>::BYTES + 6 * FRUN_BYTES);
+                if (lane == 0) mbar_expect_tx(&full[s], Q * Vec16<T>::BYTES + (NREC + 2) * FRUN_BYTES);
                 __syncwarp();
 #pragma unroll 1
                 for (int k = lane; k < NCOPY; k += 32) {
                     if (k < Q) bulk_g2s(&st->run[k][0], B + (a.run0[k] + x0), Vec16<T>::BYTES, &full[s]);
-                    else if (k < Q + 4)
+                    else if (k < Q + NREC)
                         bulk_g2s(&st->rec[k - Q][0], a.record + (a.rec0[k - Q] + x0), FRUN_BYTES, &full[s]);
-                    else if (k == Q + 4) bulk_g2s(&st->mask[0], a.mask + x0, FRUN_BYTES, &full[s]);
+                    else if (k == Q + NREC) bulk_g2s(&st->mask[0], a.mask + x0, FRUN_BYTES, &full[s]);
                     else bulk_g2s(&st->alpha[0], a.alpha + x0, FRUN_BYTES, &full[s]);
                 }
             }
@@ -105,7 +108,21 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
             }
             if (fluid) {
                 const float u[3] = {st->rec[1][a.recd[1] + c], st->rec[2][a.recd[2] + c], st->rec[3][a.recd[3] + c]};
-                const float ab = collide_vjp<Q, COLL>(v, st->rec[0][a.recd[0] + c], u, st->alpha[c], a.P);
+                const float rp = st->rec[0][a.recd[0] + c];
+                float ab = collide_vjp<Q, COLL>(v, rp, u, st->alpha[c], a.P);
+                if constexpr (STG) {
+                    if (a.stage) {
+                        // the stage seed of this state: d(w . responses)/dg from its record
+                        float Sm[6], fb[Q];
+#pragma unroll
+                        for (int e = 0; e < 6; ++e) Sm[e] = st->rec[4 + e][a.recd[4 + e] + c];
+                        const PortMap* pm = (m & MASK_PORT) ? &a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1] : nullptr;
+                        ab += response_vjp<Q>(rp, u, Sm, st->alpha[c], pm ? pm->dp_weight : 0.f, pm != nullptr, a.seed,
+                                              a.P, fb);
+#pragma unroll
+                        for (int q = 0; q < Q; ++q) v[q] += fb[q];
+                    }
+                }
                 if (a.overwrite_abar) a.abar[x] = ab * a.abar_factor;
                 else a.abar[x] = fmaf(ab, a.abar_factor, a.abar[x]);
                 if (a.port_transpose && (m & MASK_PORT)) port_transpose<Q>(a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], v);
@@ -134,17 +151,17 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
     }
 }
 
-template <int Q, int COLL, typename T, int AL>
+template <int Q, int COLL, typename T, int AL, int STG>
 cudaError_t run_adjoint_al(const AdjArgs& a, cudaStream_t s) {
-    constexpr size_t smem = pipe_bytes<AdjStage<Q, T>>();
+    constexpr size_t smem = pipe_bytes<AdjStage<Q, T, STG ? 10 : 4>>();
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = set_smem(k_adjoint<Q, COLL, T, AL>, smem);
+        cudaError_t e = set_smem(k_adjoint<Q, COLL, T, AL, STG>, smem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    const int grid = persistent_grid((const void*)k_adjoint<Q, COLL, T, AL>, a.G.n, smem, TPB, TILE);
-    k_adjoint<Q, COLL, T, AL><<<grid, TPB, smem, s>>>(a);
+    const int grid = persistent_grid((const void*)k_adjoint<Q, COLL, T, AL, STG>, a.G.n, smem, TPB, TILE);
+    k_adjoint<Q, COLL, T, AL, STG><<<grid, TPB, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -159,7 +176,10 @@ bool adj_table_is_aligned(const int32_t* rund) {
 
 template <int Q, int COLL, typename T>
 cudaError_t run_adjoint(const AdjArgs& a, cudaStream_t s) {
-    return adj_table_is_aligned<Q, T>(a.rund) ? run_adjoint_al<Q, COLL, T, 1>(a, s) : run_adjoint_al<Q, COLL, T, 0>(a, s);
+    const bool al = adj_table_is_aligned<Q, T>(a.rund);
+    if (a.rec_planes == 10)
+        return al ? run_adjoint_al<Q, COLL, T, 1, 1>(a, s) : run_adjoint_al<Q, COLL, T, 0, 1>(a, s);
+    return al ? run_adjoint_al<Q, COLL, T, 1, 0>(a, s) : run_adjoint_al<Q, COLL, T, 0, 0>(a, s);
 }
 
 }  // namespace
@@ -168,13 +188,15 @@ cudaError_t launch_adjoint(int Q, int coll, int lstorage, const AdjArgs& a0, int
     (void)grid;
     AdjArgs a = a0;
     run_table(Q, a.G, +1, lstorage == ST_F32 ? 4 : 8, a.run0, a.rund);
-    for (int k = 0; k < 4; ++k) {
+    if (a.rec_planes != 4 && a.rec_planes != 10) return cudaErrorInvalidValue;
+    for (int k = 0; k < a.rec_planes; ++k) {
         const int64_t first = (int64_t)k * a.G.n;
         a.recd[k] = (int32_t)(first % 4);
         a.rec0[k] = first - a.recd[k];
     }
     // every bulk copy needs 16-byte aligned addresses: refuse to launch otherwise
-    if (!staged_aligned(a.src, a.run0, Q, lstorage == ST_F32 ? 4 : 2) || !staged_aligned(a.record, a.rec0, 4, 4) ||
+    if (!staged_aligned(a.src, a.run0, Q, lstorage == ST_F32 ? 4 : 2) ||
+        !staged_aligned(a.record, a.rec0, a.rec_planes, 4) ||
         !staged_aligned(a.mask, nullptr, 0, 4) || !staged_aligned(a.alpha, nullptr, 0, 4))
         return cudaErrorMisalignedAddress;
     if (Q == 19) {

@@ -123,6 +123,13 @@ struct Physics {
     float proj_m2[MAX_PROJ][6];    // sum_i w_i b_i c_ia c_ib (xx yy zz xy xz yz)
 };
 
+// Weights (after the reference's scalings) and unit scales of the response
+// VJP (response_vjp in lbm_device.cuh).
+struct SeedParams {
+    float w[8];
+    float vel, dens, dt_s, tau;
+};
+
 // Per-step admission reductions (solver.rs:714-755) for one state.
 struct StepDiag {
     double mass_hi, mass_lo;  // sum of rho over fluid cells (compensated)

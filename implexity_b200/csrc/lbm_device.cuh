@@ -545,6 +545,119 @@ __device__ __forceinline__ float collide_vjp(float (&gb)[Q], float rp, const flo
     return abar;
 }
 
+// Second moments S_ab = sum_q c_a c_b g_q (xx yy zz xy xz yz) of g = f - w.
+template <int Q>
+__device__ __forceinline__ void second_moments(const float (&g)[Q], float (&S)[6]) {
+    using L = Lat<Q>;
+#pragma unroll
+    for (int e = 0; e < 6; ++e) S[e] = 0.f;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int c0 = L::cx(q), c1 = L::cy(q), c2 = L::cz(q);
+        if (c0) S[0] += g[q];
+        if (c1) S[1] += g[q];
+        if (c2) S[2] += g[q];
+        if (c0 && c1) S[3] += c0 * c1 * g[q];
+        if (c0 && c2) S[4] += c0 * c2 * g[q];
+        if (c1 && c2) S[5] += c1 * c2 * g[q];
+    }
+}
+
+// VJP of the weighted responses of one fluid cell (vector_vjp,
+// solver.rs:896-947, plus the pressure drop and the viscous dissipation
+// sigma:sigma / (2 rho nu), sigma = -(1 - omega/2) (Pi_neq + (uF + Fu)/2))
+// with respect to the cell's streamed populations g = f - w, given rho - 1,
+// the Brinkman velocity u and the second moments S of g.  fb = d/dg; returns
+// the cotangent of alpha.  The responses depend on g only through these
+// moments, so the adjoint step can seed a state from its record alone.
+template <int Q>
+__device__ __forceinline__ float response_vjp(float rp, const float (&u)[3], const float (&S)[6], float alpha,
+                                              float dpw, bool port, const SeedParams& sp, const Physics& P,
+                                              float (&fb)[Q]) {
+    using L = Lat<Q>;
+    const float k = 1.f - 0.5f / sp.tau;
+    const float nu = (sp.tau - 0.5f) / 3.f;
+    const float rho = 1.f + rp;
+    float F[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) F[d] = rho * (P.a[d] - alpha * u[d]);
+    const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+    float sig[6];
+    float ss = 0.f;
+#pragma unroll
+    for (int e = 0; e < 6; ++e) {
+        const float pi = S[e] - (e < 3 ? rp / 3.f : 0.f) - rho * u[ia[e]] * u[ib[e]];
+        const float t = 0.5f * (u[ia[e]] * F[ib[e]] + u[ib[e]] * F[ia[e]]);
+        sig[e] = -k * (pi + t);
+        ss += (e < 3 ? 1.f : 2.f) * sig[e] * sig[e];
+    }
+    // cotangents of rho, u, F, M2 (all lattice units)
+    const float V = sp.vel;
+    const float U[3] = {u[0] * V, u[1] * V, u[2] * V};
+    const float usq = U[0] * U[0] + U[1] * U[1] + U[2] * U[2];
+    const float R = rho * sp.dens;
+    const float W3 = sp.w[3], W4 = sp.w[4], W7 = sp.w[7];
+    float rb = 0.f, abar = 0.f, ub[3], Fb[3] = {0.f, 0.f, 0.f}, Sb[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float kin = W3 + W4 * alpha / sp.dt_s;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) ub[d] = sp.w[d] * V + kin * R * 2.f * U[d] * V;
+    rb += kin * sp.dens * usq;
+    abar += W4 * R / sp.dt_s * usq;
+    if (port) rb += sp.w[6] * dpw * sp.dens * V * V / 3.f;
+    if (W7 != 0.f) {
+        rb += -W7 * ss / (2.f * rho * rho * nu);
+#pragma unroll
+        for (int e = 0; e < 6; ++e) {
+            const float mult = (e < 3 ? 1.f : 2.f);  // off-diagonals appear twice
+            const float pb = -k * W7 * sig[e] / (rho * nu) * mult;
+            const int i0 = ia[e], i1 = ib[e];
+            Sb[e] += pb;
+            rb -= pb * ((e < 3 ? 1.f / 3.f : 0.f) + u[i0] * u[i1]);
+            if (e < 3) {
+                ub[i0] -= 2.f * rho * pb * u[i0];
+                ub[i0] += pb * F[i0];
+                Fb[i0] += pb * u[i0];
+            } else {
+                ub[i0] -= rho * pb * u[i1];
+                ub[i1] -= rho * pb * u[i0];
+                ub[i0] += 0.5f * pb * F[i1];
+                ub[i1] += 0.5f * pb * F[i0];
+                Fb[i1] += 0.5f * pb * u[i0];
+                Fb[i0] += 0.5f * pb * u[i1];
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        rb += Fb[d] * (P.a[d] - alpha * u[d]);
+        abar -= Fb[d] * rho * u[d];
+        ub[d] -= Fb[d] * rho * alpha;
+    }
+    const float s = 1.f + 0.5f * alpha;
+    const float inv = 1.f / (s * rho);
+    float mb[3], sbar = 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        mb[d] = ub[d] * inv;
+        rb -= ub[d] * (s * u[d] - 0.5f * P.a[d]) * inv;
+        sbar -= ub[d] * u[d] / s;
+    }
+    abar += 0.5f * sbar;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int c0 = L::cx(q), c1 = L::cy(q), c2 = L::cz(q);
+        float v = rb;
+        if (c0) v += c0 * mb[0] + Sb[0];
+        if (c1) v += c1 * mb[1] + Sb[1];
+        if (c2) v += c2 * mb[2] + Sb[2];
+        if (c0 && c1) v += c0 * c1 * Sb[3];
+        if (c0 && c2) v += c0 * c2 * Sb[4];
+        if (c1 && c2) v += c1 * c2 * Sb[5];
+        fb[q] = v;
+    }
+    return abar;
+}
+
 // ------------------------------------------------------------------ reductions
 __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
     s = a + b;

@@ -137,6 +137,15 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
                     }
                 }
                 const float mn = a.diag ? min_population<Q, SC>(v) : 0.f;
+                if (a.record && a.record_s) {
+                    // second moments of g for the stage seeds of the adjoint
+                    float g[Q], S[6];
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) g[q] = SC ? L::w(q) * v[q] : v[q];
+                    second_moments<Q>(g, S);
+#pragma unroll
+                    for (int e = 0; e < 6; ++e) a.record[(size_t)(4 + e) * n + x] = S[e];
+                }
                 const Macro M = collide_fused<Q, COLL, SC>(v, alpha, a.P, a.collide);
                 if (a.diag) {
                     acc.mass += M.rp;

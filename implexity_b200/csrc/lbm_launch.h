@@ -31,6 +31,7 @@ struct FwdArgs {
     StepDiag* diag;          // per-state admission output (nullptr: off)
     Reduce red;
     float* record;           // (rho-1, ux, uy, uz) planes (nullptr: off)
+    int32_t record_s;        // also record the six second moments of g (planes 4..9)
     int32_t collide;         // 0: only load/diag/record (no collision, no store)
     int32_t bulk_store;      // full tiles leave through bulk stores (planes 16-byte aligned)
     uint32_t step;           // absolute step index (seeds the stochastic rounding)
@@ -50,7 +51,10 @@ struct AdjArgs {
     const uint32_t* mask;
     const float* alpha;
     const PortMap* ports;
-    const float* record;     // (rho-1, ux, uy, uz) of the forward state
+    const float* record;     // (rho-1, ux, uy, uz[, S xx yy zz xy xz yz]) of the forward state
+    int32_t rec_planes;      // 4, or 10 with the second moments (stage seeds)
+    int32_t stage;           // add the response VJP of this state (stage objective)
+    SeedParams seed;         // weights and scales of that VJP
     float* abar;             // accumulated alpha cotangent
     int32_t port_transpose;  // store Ports^T lambda (1) or lambda itself (0)
     int32_t overwrite_abar;  // abar = (1) or += (0)
@@ -62,8 +66,8 @@ struct AdjArgs {
     int* err;                // set when a bounded wait gave up
     int64_t run0[27];        // staged adjoint runs (see FwdArgs)
     int32_t rund[27];
-    int64_t rec0[4];         // staged record runs
-    int32_t recd[4];
+    int64_t rec0[10];        // staged record runs
+    int32_t recd[10];
 };
 
 struct ObjArgs {

@@ -40,8 +40,6 @@ __global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
     Sums<8> acc;
     acc.init();
     double nsum = 0.0;
-    const float k = 1.f - 0.5f / a.tau;
-    const float nu = (a.tau - 0.5f) / 3.f;
     for (uint32_t x = blockIdx.x * BLOCK + threadIdx.x; x < (uint32_t)n; x += gridDim.x * BLOCK) {
         const uint32_t m = a.mask[x];
         if (m & MASK_SOLID) {
@@ -128,97 +126,19 @@ __global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
         }
         if (a.apply_ports && pm) apply_port<Q>(*pm, g);
         Macro M = macroscopic<Q>(g, alpha, a.P);
-        // second moments of g: M2_ab = sum c_a c_b g (f adds delta/3)
-        float S[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float S[6];
+        second_moments<Q>(g, S);
+        SeedParams sp;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const int c0 = L::cx(q), c1 = L::cy(q), c2 = L::cz(q);
-            if (c0) S[0] += g[q];
-            if (c1) S[1] += g[q];
-            if (c2) S[2] += g[q];
-            if (c0 && c1) S[3] += c0 * c1 * g[q];
-            if (c0 && c2) S[4] += c0 * c2 * g[q];
-            if (c1 && c2) S[5] += c1 * c2 * g[q];
-        }
+        for (int r = 0; r < 8; ++r) sp.w[r] = (float)a.w[r];
+        sp.vel = a.vel;
+        sp.dens = a.dens;
+        sp.dt_s = a.dt_s;
+        sp.tau = a.tau;
         const float* u = M.u;
-        const float* F = M.F;
-        const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
-        float sig[6];
-        float ss = 0.f;
-#pragma unroll
-        for (int e = 0; e < 6; ++e) {
-            const float pi = S[e] - (e < 3 ? M.rp / 3.f : 0.f) - M.rho * u[ia[e]] * u[ib[e]];
-            const float t = 0.5f * (u[ia[e]] * F[ib[e]] + u[ib[e]] * F[ia[e]]);
-            sig[e] = -k * (pi + t);
-            ss += (e < 3 ? 1.f : 2.f) * sig[e] * sig[e];
-        }
-        const float dpw = pm ? pm->dp_weight : 0.f;
         {
-            // cotangents of rho, u, F, M2 (all lattice units)
-            const float V = a.vel;
-            const float U[3] = {u[0] * V, u[1] * V, u[2] * V};
-            const float usq = U[0] * U[0] + U[1] * U[1] + U[2] * U[2];
-            const float R = M.rho * a.dens;
-            const float W3 = (float)a.w[3], W4 = (float)a.w[4], W7 = (float)a.w[7];
-            float rb = 0.f, abar = 0.f, ub[3], Fb[3] = {0.f, 0.f, 0.f}, Sb[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            const float kin = W3 + W4 * alpha / a.dt_s;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) ub[d] = (float)a.w[d] * V + kin * R * 2.f * U[d] * V;
-            rb += kin * a.dens * usq;
-            abar += W4 * R / a.dt_s * usq;
-            if (pm) rb += (float)a.w[6] * dpw * a.dens * V * V / 3.f;
-            if (W7 != 0.f) {
-                rb += -W7 * ss / (2.f * M.rho * M.rho * nu);
-#pragma unroll
-                for (int e = 0; e < 6; ++e) {
-                    const float mult = (e < 3 ? 1.f : 2.f);  // off-diagonals appear twice
-                    const float pb = -k * W7 * sig[e] / (M.rho * nu) * mult;
-                    const int i0 = ia[e], i1 = ib[e];
-                    Sb[e] += pb;
-                    rb -= pb * ((e < 3 ? 1.f / 3.f : 0.f) + u[i0] * u[i1]);
-                    if (e < 3) {
-                        ub[i0] -= 2.f * M.rho * pb * u[i0];
-                        ub[i0] += pb * F[i0];
-                        Fb[i0] += pb * u[i0];
-                    } else {
-                        ub[i0] -= M.rho * pb * u[i1];
-                        ub[i1] -= M.rho * pb * u[i0];
-                        ub[i0] += 0.5f * pb * F[i1];
-                        ub[i1] += 0.5f * pb * F[i0];
-                        Fb[i1] += 0.5f * pb * u[i0];
-                        Fb[i0] += 0.5f * pb * u[i1];
-                    }
-                }
-            }
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                rb += Fb[d] * (a.P.a[d] - alpha * u[d]);
-                abar -= Fb[d] * M.rho * u[d];
-                ub[d] -= Fb[d] * M.rho * alpha;
-            }
-            const float s = 1.f + 0.5f * alpha;
-            const float inv = 1.f / (s * M.rho);
-            float mb[3], sbar = 0.f;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                mb[d] = ub[d] * inv;
-                rb -= ub[d] * (s * u[d] - 0.5f * a.P.a[d]) * inv;
-                sbar -= ub[d] * u[d] / s;
-            }
-            abar += 0.5f * sbar;
             float fb[Q];
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const int c0 = L::cx(q), c1 = L::cy(q), c2 = L::cz(q);
-                float v = rb;
-                if (c0) v += c0 * mb[0] + Sb[0];
-                if (c1) v += c1 * mb[1] + Sb[1];
-                if (c2) v += c2 * mb[2] + Sb[2];
-                if (c0 && c1) v += c0 * c1 * Sb[3];
-                if (c0 && c2) v += c0 * c2 * Sb[4];
-                if (c1 && c2) v += c1 * c2 * Sb[5];
-                fb[q] = v;
-            }
+            const float abar = response_vjp<Q>(M.rp, M.u, S, alpha, pm ? pm->dp_weight : 0.f, pm != nullptr, sp, a.P, fb);
             a.abar_final[x] = abar;
             a.phibar[x] = (float)a.w[5];
             if (a.record) {

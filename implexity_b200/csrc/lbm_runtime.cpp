@@ -166,7 +166,36 @@ struct PortSpec {
     int axis, sign;
     double vel[3];
     double density;
+    // pulsatile signal (moving/boundary.rs:98-126): value(t) = ramp(t) (wave(t) amplitude + mean)
+    bool pulsatile = false;
+    double mean_vel[3] = {0, 0, 0}, amp_vel[3] = {0, 0, 0};  // lattice units
+    double mean_rho = 1.0, amp_rho = 0.0;                     // lattice density (mean includes 1)
+    double freq = 0, phase = 0, ramp = 0;
 };
+
+// Signal::factors (moving/boundary.rs:111-125): the C2 smoothstep ramp and
+// the sine wave at time t seconds.
+void signal_factors(const PortSpec& p, double t, double& ramp, double& wave) {
+    ramp = 1.0;
+    if (p.ramp > 0.0 && t < p.ramp) {
+        double s = t / p.ramp;
+        if (s < 0.0) s = 0.0;
+        ramp = s * s * s * (10.0 - s * 15.0 + s * s * 6.0);
+    }
+    wave = p.freq == 0.0 ? 0.0 : std::sin(t * (2.0 * M_PI * p.freq) + p.phase);
+}
+
+// The port's values for the reconstruction producing the state at time t
+// seconds (moving/field.rs:1002-1013).
+PortSpec spec_at(const PortSpec& p, double t) {
+    PortSpec q = p;
+    if (!p.pulsatile) return q;
+    double ramp, wave;
+    signal_factors(p, t, ramp, wave);
+    for (int d = 0; d < 3; ++d) q.vel[d] = ramp * (wave * p.amp_vel[d] + p.mean_vel[d]);
+    if (p.pressure) q.density = 1.0 + ramp * (wave * p.amp_rho + (p.mean_rho - 1.0));
+    return q;
+}
 
 void reconstruct(const HostLat& L, const PortSpec& p, const double a[3], const double* f, double* out) {
     const int Q = L.Q;
@@ -306,6 +335,18 @@ struct lbm_handle {
     DevBuf pop, mask, alpha, phi, raw, den, slope, cls_d, fixed_d, offsets_d, ports_d, partial, counter, diag;
     DevBuf lam, record, abar, abar_final, phibar, scale, grad, norm2, sums, scratch, errflag;
     int lam_storage = LBM_STORE_F32;
+    // --- ports: normalised specs with their signals; pulsatile ports keep one
+    // set of maps per state index on the device (ensure_port_maps)
+    std::vector<PortSpec> port_specs;
+    bool pulsatile = false;
+    int64_t map_states = 0;
+    std::vector<PortMap> maps_host;
+    // --- stage objective: the responses of every state of the last forward
+    bool time_average = false;
+    DevBuf tsums;
+    double tavg[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool tavg_valid = false;
+    int64_t peak_extra = 0;  // second-level checkpoint bytes of the last horizon gradient
     std::vector<Checkpoint> ckpts;
     std::vector<StepDiag> last_trajectory;
     // --- state
@@ -343,6 +384,61 @@ void require(bool ok, const char* msg) {
     if (!ok) throw ContractError(msg);
 }
 bool finite_positive(double v) { return std::isfinite(v) && v > 0; }
+
+// The affine port maps (shifted variables) of every port for the values in
+// force at time t seconds: bias and Jacobian of the FP64 reconstruction over
+// the unknown populations, tabulated at the weights.
+std::vector<PortMap> port_maps_at(const lbm_handle& h, double t_s) {
+    std::vector<PortMap> maps(h.port_specs.size());
+    const int Q = h.Q;
+    for (size_t k = 0; k < h.port_specs.size(); ++k) {
+        const PortSpec spec = spec_at(h.port_specs[k], t_s);
+        PortMap& M = maps[k];
+        std::memset(&M, 0, sizeof(M));
+        double base[27] = {}, pert[27] = {}, r0[27] = {}, r1[27] = {};
+        for (int q = 0; q < Q; ++q) base[q] = h.L.w[q];
+        reconstruct(h.L, spec, h.a, base, r0);
+        for (int q = 0; q < Q; ++q)
+            if (h.L.c[q][spec.axis] == spec.sign) M.unknown_mask |= 1u << q;
+        for (int r = 0; r < Q; ++r)
+            if (M.unknown_mask & (1u << r)) M.bias[r] = (float)(r0[r] - h.L.w[r]);
+        for (int kq = 0; kq < Q; ++kq) {
+            for (int q = 0; q < Q; ++q) pert[q] = base[q];
+            pert[kq] += 1.0;
+            reconstruct(h.L, spec, h.a, pert, r1);
+            for (int r = 0; r < Q; ++r)
+                if (M.unknown_mask & (1u << r)) M.jac[r][kq] = (float)(r1[r] - r0[r]);
+        }
+        const bool both = h.n_inlet > 0 && h.n_outlet > 0;
+        M.dp_weight = !both ? 0.f : spec.pressure ? (float)(-1.0 / h.n_outlet) : (float)(1.0 / h.n_inlet);
+    }
+    return maps;
+}
+
+// Pulsatile ports: the maps of the reconstructions producing states
+// 0..t_max (state t at time t * step_s) are on the device afterwards.
+void ensure_port_maps(lbm_handle& h, int64_t t_max) {
+    if (!h.pulsatile || t_max < h.map_states) return;
+    const int64_t states = std::max<int64_t>({t_max + 1, 2 * h.map_states, h.step_count + 1});
+    h.maps_host.resize((size_t)states * h.n_ports);
+    for (int64_t t = h.map_states; t < states; ++t) {
+        const std::vector<PortMap> m = port_maps_at(h, (double)t * h.dt);
+        std::copy(m.begin(), m.end(), h.maps_host.begin() + (size_t)t * h.n_ports);
+    }
+    // kernels queued on the stream may still read the old table
+    CK(cudaStreamSynchronize(h.stream));
+    h.ports_d.reset();
+    h.ports_d.alloc(h.maps_host.size() * sizeof(PortMap), &h.device_bytes);
+    CK(cudaMemcpy(h.ports_d.p, h.maps_host.data(), h.maps_host.size() * sizeof(PortMap), cudaMemcpyHostToDevice));
+    h.map_states = states;
+}
+
+// Device port maps in force when state t is loaded.
+const PortMap* ports_at(lbm_handle& h, int64_t t) {
+    if (!h.pulsatile) return h.ports_d.as<PortMap>();
+    ensure_port_maps(h, t);
+    return h.ports_d.as<PortMap>() + (size_t)t * h.n_ports;
+}
 
 void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
     // solver.rs:414-550 in order; key-set and array-shape checks belong to the
@@ -501,16 +597,37 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
         for (int d = 0; d < 3; ++d) s.vel[d] = pt.velocity_m_s[d] * p.step_s / p.spacing_m;
         require(!(s.pressure && pt.velocity_m_s[s.axis] != 0.0),
                 "Pressure port velocity specifies tangential components only; normal component must be zero");
-        double un = std::sqrt(s.vel[0] * s.vel[0] + s.vel[1] * s.vel[1] + s.vel[2] * s.vel[2]);
-        require(!(un * std::sqrt(3.0) > p.mach_limit), "Authored port velocity exceeds Mach limit");
+        // pulsatile signal (keys of implexity-physics-fsi problem/fluid.rs:256-322)
+        require(std::isfinite(pt.frequency_hz) && pt.frequency_hz >= 0.0, "Port frequency_hz must be nonnegative");
+        require(std::isfinite(pt.phase_rad), "Port phase_rad must be finite");
+        require(std::isfinite(pt.ramp_s) && pt.ramp_s >= 0.0, "Port ramp_s must be nonnegative");
+        s.freq = pt.frequency_hz;
+        s.phase = pt.phase_rad;
+        s.ramp = pt.ramp_s;
+        s.pulsatile = s.freq != 0.0 || s.ramp != 0.0;
+        for (int d = 0; d < 3; ++d) {
+            require(std::isfinite(pt.amplitude_m_s[d]), "Port amplitude_m_s requires three finite components");
+            s.mean_vel[d] = s.vel[d];
+            s.amp_vel[d] = s.pressure ? 0.0 : pt.amplitude_m_s[d] * p.step_s / p.spacing_m;
+        }
+        // the largest speed the signal reaches (moving/field.rs:884)
+        double un2 = 0.0;
+        for (int d = 0; d < 3; ++d) un2 += std::pow(std::fabs(s.mean_vel[d]) + std::fabs(s.amp_vel[d]), 2);
+        require(!(std::sqrt(un2) * std::sqrt(3.0) > p.mach_limit), "Authored port velocity exceeds Mach limit");
         s.density = 1.0;
         if (s.pressure) {
             require(std::isfinite(pt.gauge_pressure_Pa), "Finite scalar gauge pressure required");
+            require(std::isfinite(pt.amplitude_Pa), "Port amplitude_Pa must be finite");
             double unit = p.spacing_m / p.step_s;
-            double rho = 1.0 + pt.gauge_pressure_Pa * 3.0 / (p.density_kg_m3 * unit * unit);
-            require(rho >= 0.9 && rho <= 1.1, "Pressure port density must remain within 10% of reference");
+            const double to_rho = 3.0 / (p.density_kg_m3 * unit * unit);
+            double rho = 1.0 + pt.gauge_pressure_Pa * to_rho;
+            const double swing = std::fabs(pt.amplitude_Pa) * to_rho;
+            require(rho - swing >= 0.9 && rho + swing <= 1.1, "Pressure port density must remain within 10% of reference");
             s.density = rho;
+            s.mean_rho = rho;
+            s.amp_rho = pt.amplitude_Pa * to_rho;
         }
+        if (s.pulsatile) s = spec_at(s, 0.0);
         for (int64_t x : cells) used[x] = 1;
         specs.push_back(s);
         port_cells.push_back(cells);
@@ -519,29 +636,12 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
     h.n_inlet = h.n_outlet = 0;
     for (size_t k = 0; k < specs.size(); ++k) (specs[k].pressure ? h.n_outlet : h.n_inlet) += (int64_t)port_cells[k].size();
 
-    // port affine maps in shifted variables
-    std::vector<PortMap> maps(specs.size());
-    for (size_t k = 0; k < specs.size(); ++k) {
-        PortMap& M = maps[k];
-        std::memset(&M, 0, sizeof(M));
-        const int Q = h.Q;
-        double base[27], pert[27], r0[27], r1[27];
-        for (int q = 0; q < Q; ++q) base[q] = h.L.w[q];
-        reconstruct(h.L, specs[k], h.a, base, r0);
-        for (int q = 0; q < Q; ++q)
-            if (h.L.c[q][specs[k].axis] == specs[k].sign) M.unknown_mask |= 1u << q;
-        for (int r = 0; r < Q; ++r)
-            if (M.unknown_mask & (1u << r)) M.bias[r] = (float)(r0[r] - h.L.w[r]);
-        for (int kq = 0; kq < Q; ++kq) {
-            for (int q = 0; q < Q; ++q) pert[q] = base[q];
-            pert[kq] += 1.0;
-            reconstruct(h.L, specs[k], h.a, pert, r1);
-            for (int r = 0; r < Q; ++r)
-                if (M.unknown_mask & (1u << r)) M.jac[r][kq] = (float)(r1[r] - r0[r]);
-        }
-        bool both = h.n_inlet > 0 && h.n_outlet > 0;
-        M.dp_weight = !both ? 0.f : specs[k].pressure ? (float)(-1.0 / h.n_outlet) : (float)(1.0 / h.n_inlet);
-    }
+    // port affine maps in shifted variables (for pulsatile ports: one set per
+    // state index, built on demand by ensure_port_maps)
+    h.port_specs = specs;
+    h.pulsatile = false;
+    for (const PortSpec& sp : specs) h.pulsatile = h.pulsatile || sp.pulsatile;
+    std::vector<PortMap> maps = port_maps_at(h, 0.0);
 
     // link masks (Streaming::new, solver.rs:84-119)
     std::vector<uint32_t> mask(n, 0);
@@ -653,6 +753,8 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
     CK(cudaMemsetAsync(h.errflag.p, 0, sizeof(int), h.stream));
     CK(cudaMemsetAsync(h.pop.p, 0, h.pop.bytes, h.stream));
     CK(cudaStreamSynchronize(h.stream));
+    h.time_average = p.time_average != 0;
+    if (h.pulsatile) ensure_port_maps(h, h.step_count);
 }
 
 // ------------------------------------------------------------ stepping
@@ -673,7 +775,7 @@ FwdArgs fwd_args(lbm_handle& h) {
     a.bulk_store = h.G.n % (int64_t)(16 / storage_bytes(h.storage)) == 0 ? 1 : 0;
     a.mask = h.mask.as<uint32_t>();
     a.alpha = h.alpha.as<float>();
-    a.ports = h.ports_d.as<PortMap>();
+    a.ports = ports_at(h, h.t);
     a.red = reduce_of(h);
     a.err = h.errflag.as<int>();
     return a;
@@ -682,11 +784,12 @@ FwdArgs fwd_args(lbm_handle& h) {
 int coll_kind(const lbm_handle& h) { return h.coll == LBM_MRT ? CK_MRT : CK_PAIRS; }
 
 // One step of the current state; diag / record optional.
-void step(lbm_handle& h, StepDiag* diag, float* record) {
+void step(lbm_handle& h, StepDiag* diag, float* record, bool record_s = false) {
     FwdArgs a = fwd_args(h);
     a.apply_ports = h.pending ? 1 : 0;
     a.diag = diag;
     a.record = record;
+    a.record_s = record_s ? 1 : 0;
     a.collide = 1;
     a.step = (uint32_t)h.t;
     CK(launch_forward(h.Q, coll_kind(h), h.storage, a, grid_for(h), h.stream));
@@ -696,12 +799,13 @@ void step(lbm_handle& h, StepDiag* diag, float* record) {
 }
 
 // Load-only pass of the current state (admission reductions and/or record).
-void inspect(lbm_handle& h, StepDiag* diag, float* record) {
+void inspect(lbm_handle& h, StepDiag* diag, float* record, bool record_s = false) {
     FwdArgs a = fwd_args(h);
     a.dst = nullptr;
     a.apply_ports = h.pending ? 1 : 0;
     a.diag = diag;
     a.record = record;
+    a.record_s = record_s ? 1 : 0;
     a.collide = 0;
     CK(launch_forward(h.Q, coll_kind(h), h.storage, a, grid_for(h), h.stream));
 }
@@ -787,11 +891,19 @@ void check_errflag(lbm_handle& h) {
 
 // Runs `steps` steps from the current state with admission of every state
 // including the current one.  Optionally stores checkpoints every K steps.
-lbm_status run_admitted(lbm_handle& h, int64_t steps, lbm_diag_t* out, int64_t K) {
+void stage_sums(lbm_handle& h, double* slot);
+void finish_time_average(lbm_handle& h, int64_t steps);
+
+// With `averages`, the responses of every state 1..steps are summed on the
+// device as well (the stage objective's value, lbm_time_average).
+lbm_status run_admitted(lbm_handle& h, int64_t steps, lbm_diag_t* out, int64_t K, bool averages = false) {
     require_design(h);
     int64_t* ctr = &h.device_bytes;
     h.diag.alloc((size_t)(steps + 1) * sizeof(StepDiag), ctr);
     StepDiag* d = h.diag.as<StepDiag>();
+    ensure_port_maps(h, h.t + steps);
+    h.tavg_valid = false;
+    if (averages) h.tsums.alloc((size_t)(steps + 1) * 16 * sizeof(double), ctr);
     CK(cudaEventRecord(h.ev0, h.stream));
     for (int64_t s = 0; s < steps; ++s) {
         if (K > 0 && s % K == 0) {
@@ -806,6 +918,7 @@ lbm_status run_admitted(lbm_handle& h, int64_t steps, lbm_diag_t* out, int64_t K
             h.ckpts.push_back(std::move(c));
         }
         step(h, d + s, nullptr);
+        if (averages) stage_sums(h, h.tsums.as<double>() + (size_t)(s + 1) * 16);
     }
     inspect(h, d + steps, nullptr);
     CK(cudaEventRecord(h.ev1, h.stream));
@@ -816,6 +929,7 @@ lbm_status run_admitted(lbm_handle& h, int64_t steps, lbm_diag_t* out, int64_t K
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, h.ev0, h.ev1));
     check_errflag(h);
+    if (averages) finish_time_average(h, steps);
     return admit(h, hd, out, ms);
 }
 
@@ -829,7 +943,7 @@ ObjArgs obj_args(lbm_handle& h) {
     a.mask = h.mask.as<uint32_t>();
     a.alpha = h.alpha.as<float>();
     a.phi = h.phi.as<float>();
-    a.ports = h.ports_d.as<PortMap>();
+    a.ports = ports_at(h, h.t);
     a.apply_ports = h.pending ? 1 : 0;
     a.tau = (float)h.tau;
     a.vel = (float)(h.dx / h.dt);
@@ -841,14 +955,8 @@ ObjArgs obj_args(lbm_handle& h) {
 
 double visc_scale(const lbm_handle& h) { return h.density * std::pow(h.dx, 5) / std::pow(h.dt, 3); }
 
-void responses(lbm_handle& h, double* out8, float* fields) {
-    ObjArgs a = obj_args(h);
-    a.sums = h.sums.as<double>();
-    a.fields = fields;
-    CK(launch_objective(h.Q, h.storage, LBM_STORE_F32, 0, a, grid_for(h), h.stream));
-    double s[16];
-    CK(cudaMemcpyAsync(s, h.sums.p, sizeof(s), cudaMemcpyDeviceToHost, h.stream));
-    CK(cudaStreamSynchronize(h.stream));
+// The 8 responses from the 8 compensated sums of the objective kernel.
+void sums_to_responses(const lbm_handle& h, const double* s, double* out8) {
     double v[8];
     for (int k = 0; k < 8; ++k) v[k] = s[2 * k] + s[2 * k + 1];
     const double nf = (double)h.fluid_cells, dv = h.dx * h.dx * h.dx;
@@ -860,6 +968,37 @@ void responses(lbm_handle& h, double* out8, float* fields) {
     out8[5] = v[5] * dv;
     out8[6] = (h.n_inlet > 0 && h.n_outlet > 0) ? v[6] : 0.0;
     out8[7] = v[7] * visc_scale(h);
+}
+
+void responses(lbm_handle& h, double* out8, float* fields) {
+    ObjArgs a = obj_args(h);
+    a.sums = h.sums.as<double>();
+    a.fields = fields;
+    CK(launch_objective(h.Q, h.storage, LBM_STORE_F32, 0, a, grid_for(h), h.stream));
+    double s[16];
+    CK(cudaMemcpyAsync(s, h.sums.p, sizeof(s), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    sums_to_responses(h, s, out8);
+}
+
+// Responses of the current state, summed into a device slot (16 doubles).
+void stage_sums(lbm_handle& h, double* slot) {
+    ObjArgs a = obj_args(h);
+    a.sums = slot;
+    CK(launch_objective(h.Q, h.storage, LBM_STORE_F32, 0, a, grid_for(h), h.stream));
+}
+
+// Mean of the responses of states 1..steps (slots filled by stage_sums).
+void finish_time_average(lbm_handle& h, int64_t steps) {
+    std::vector<double> all((size_t)(steps + 1) * 16);
+    CK(cudaMemcpy(all.data(), h.tsums.p, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0}, r[8];
+    for (int64_t t = 1; t <= steps; ++t) {
+        sums_to_responses(h, all.data() + (size_t)t * 16, r);
+        for (int k = 0; k < 8; ++k) acc[k] += r[k];
+    }
+    for (int k = 0; k < 8; ++k) h.tavg[k] = steps > 0 ? acc[k] / (double)steps : 0.0;
+    h.tavg_valid = steps > 0;
 }
 
 DesignArgs design_args(lbm_handle& h) {
@@ -918,7 +1057,8 @@ AdjArgs adj_args(lbm_handle& h) {
     a.dst = h.lamB();
     a.mask = h.mask.as<uint32_t>();
     a.alpha = h.alpha.as<float>();
-    a.ports = h.ports_d.as<PortMap>();
+    a.ports = ports_at(h, h.t);
+    a.rec_planes = 4;
     a.abar = h.abar.as<float>();
     a.red = reduce_of(h);
     a.err = h.errflag.as<int>();
@@ -927,9 +1067,14 @@ AdjArgs adj_args(lbm_handle& h) {
 
 // One transposed step linearised at record slot `rec`; returns nothing, the
 // norm (if requested) lands in norm2[0..1].
-void adjoint_step(lbm_handle& h, AdjState& st, const float* rec, bool want_norm) {
+void adjoint_step(lbm_handle& h, AdjState& st, const float* rec, bool want_norm, int64_t t_state = -1,
+                  const SeedParams* stage = nullptr, int rec_planes = 4) {
     AdjArgs a = adj_args(h);
     a.record = rec;
+    a.rec_planes = rec_planes;
+    a.ports = ports_at(h, t_state >= 0 ? t_state : h.t);
+    a.stage = stage ? 1 : 0;
+    if (stage) a.seed = *stage;
     a.port_transpose = 1;
     a.overwrite_abar = st.first ? 1 : 0;
     a.in_scale_inv = 1.f / st.scale;
@@ -952,22 +1097,44 @@ double read_norm(lbm_handle& h) {
 
 // Objective VJP at the current state: lambda seed, abar_final, phibar and
 // the (rho, u) record.  Returns |mu_0| (true units).
-double seed(lbm_handle& h, const double* w, AdjState& st, float* record) {
+// The weights of vector_vjp after the reference's response scalings
+// (solver.rs:896-947); every weight but the fluid volume's is multiplied by
+// `scale` (1/T for a state of a time average: the fluid volume does not
+// change in time, so its mean is itself).
+void response_weights(const lbm_handle& h, const double* w, double scale, double* out8) {
+    const double nf = (double)h.fluid_cells, dv = h.dx * h.dx * h.dx;
+    out8[0] = scale * w[0] / nf;
+    out8[1] = scale * w[1] / nf;
+    out8[2] = scale * w[2] / nf;
+    out8[3] = scale * 0.5 * w[3] * dv;
+    out8[4] = scale * w[4] * dv;
+    out8[5] = w[5] * dv;
+    out8[6] = (h.n_inlet > 0 && h.n_outlet > 0) ? scale * w[6] : 0.0;
+    out8[7] = scale * w[7] * visc_scale(h);
+}
+
+// Stage seed parameters of the adjoint kernel (the response VJP of one state).
+SeedParams stage_seed(const lbm_handle& h, const double* w, double scale) {
+    double ws[8];
+    response_weights(h, w, scale, ws);
+    SeedParams sp{};
+    for (int k = 0; k < 8; ++k) sp.w[k] = (float)ws[k];
+    sp.w[5] = 0.f;  // phi enters through phibar, seeded once
+    sp.vel = (float)(h.dx / h.dt);
+    sp.dens = (float)h.density;
+    sp.dt_s = (float)h.dt;
+    sp.tau = (float)h.tau;
+    return sp;
+}
+
+double seed(lbm_handle& h, const double* w, AdjState& st, float* record, double stage_scale = 1.0) {
     int64_t* ctr = &h.device_bytes;
     const int64_t n = h.n();
     h.abar_final.alloc((size_t)n * 4, ctr);
     h.phibar.alloc((size_t)n * 4, ctr);
     h.norm2.alloc(2 * sizeof(double), ctr);
     ObjArgs a = obj_args(h);
-    const double nf = (double)h.fluid_cells, dv = h.dx * h.dx * h.dx;
-    a.w[0] = w[0] / nf;
-    a.w[1] = w[1] / nf;
-    a.w[2] = w[2] / nf;
-    a.w[3] = 0.5 * w[3] * dv;
-    a.w[4] = w[4] * dv;
-    a.w[5] = w[5] * dv;
-    a.w[6] = (h.n_inlet > 0 && h.n_outlet > 0) ? w[6] : 0.0;
-    a.w[7] = w[7] * visc_scale(h);
+    response_weights(h, w, stage_scale, a.w);
     a.lam = h.lamA();
     a.abar_final = h.abar_final.as<float>();
     a.phibar = h.phibar.as<float>();
@@ -1097,12 +1264,32 @@ lbm_status gradient_horizon(lbm_handle& h, const double* w, const lbm_adjoint_op
         while (K * K < T) ++K;
     }
     K = std::min(K, T);
+    // the stage objective (time average over states 1..T) seeds every state;
+    // its records carry the second moments as well
+    const bool stage = o.objective == LBM_OBJ_TIME_AVERAGE;
+    const int rec_planes = stage ? 10 : 4;
     alloc_adjoint(h, o.lambda_storage);
     int64_t* ctr = &h.device_bytes;
-    const size_t rec_bytes = (size_t)h.n() * 4 * sizeof(float);
-    if (o.record_budget_bytes > 0 && (int64_t)(rec_bytes * K) > o.record_budget_bytes)
-        throw ContractError("checkpoint interval needs more record memory than record_budget_bytes");
-    h.record.alloc(rec_bytes * (size_t)K + CELL_PAD * sizeof(float), ctr);
+    const size_t rec_bytes = (size_t)h.n() * rec_planes * sizeof(float);
+    // Records for KR steps.  When a segment's K records do not fit (the
+    // caller's record budget, or ~80% of the device memory left after the
+    // T/K checkpoints), a second checkpoint level splits each segment into
+    // spans of KR steps: the segment is recomputed once storing a state every
+    // KR steps, then each span once more with its records (scan.rs Every(K)
+    // nested in itself; one more recomputed forward).
+    int64_t KR = K;
+    {
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        const size_t ab = h.array_bytes(h.storage);
+        const double ckpt_bytes = (double)((T + K - 1) / K + 2) * (double)ab;
+        double budget = 0.8 * ((double)free_b - ckpt_bytes) - (double)(1ull << 30);
+        if (o.record_budget_bytes > 0) budget = std::min(budget, (double)o.record_budget_bytes);
+        const int64_t fit = budget > 0 ? (int64_t)(budget / (double)rec_bytes) : 0;
+        if (fit < 1) throw ContractError("checkpoint interval needs more record memory than record_budget_bytes");
+        KR = std::min(K, fit);
+    }
+    h.record.alloc(rec_bytes * (size_t)KR + CELL_PAD * sizeof(float), ctr);
     h.ckpts.clear();
     // forward with checkpoints, then admission (the reference re-runs parts())
     init_state(h);
@@ -1113,37 +1300,34 @@ lbm_status gradient_horizon(lbm_handle& h, const double* w, const lbm_adjoint_op
     run_admitted(h, T, &dg, K);
     h.forward_done = true;
     AdjState st;
-    const double n0 = seed(h, w, st, nullptr);
+    const double n0 = seed(h, w, st, nullptr, stage ? 1.0 / (double)T : 1.0);
+    const SeedParams sp = stage_seed(h, w, 1.0 / (double)T);
     float* rec = h.record.as<float>();
-    const size_t rec_stride = (size_t)h.n() * 4;
+    const size_t rec_stride = (size_t)h.n() * rec_planes;
     int64_t recomputed = 0;
     float ms_fwd = 0, ms_adj = 0;
-    if (n0 > 0) {
+    if (n0 > 0 || stage) {
         cudaEvent_t ea0, ea1;
         CK(cudaEventCreate(&ea0));
         CK(cudaEventCreate(&ea1));
-        for (int64_t ci = (int64_t)h.ckpts.size() - 1; ci >= 0; --ci) {
-            Checkpoint& c = h.ckpts[ci];
-            const int64_t start = c.t, end = std::min(start + K, T);
-            CK(cudaMemcpyAsync(h.pop_array(h.cur), c.buf->p, c.buf->bytes, cudaMemcpyDeviceToDevice, h.stream));
-            h.pending = c.pending;
-            h.t = c.t;
+        int64_t peak_sub = 0;
+        // records of states [s0, e0), then their transposed steps in reverse
+        auto reverse_span = [&](int64_t s0, int64_t e0, int64_t seg_start) {
             CK(cudaEventRecord(ef0, h.stream));
-            for (int64_t t = start; t < end; ++t) {
-                float* r = rec + (size_t)(t - start) * rec_stride;
-                if (t + 1 < end) {
-                    step(h, nullptr, r);
+            for (int64_t t = s0; t < e0; ++t) {
+                float* r = rec + (size_t)(t - s0) * rec_stride;
+                if (t + 1 < e0) {
+                    step(h, nullptr, r, stage);
                     ++recomputed;
                 } else {
-                    inspect(h, nullptr, r);
+                    inspect(h, nullptr, r, stage);
                 }
             }
             CK(cudaEventRecord(ef1, h.stream));
             CK(cudaEventRecord(ea0, h.stream));
-            for (int64_t t = end - 1; t >= start; --t) {
-                const bool last = (t == start);
-                adjoint_step(h, st, rec + (size_t)(t - start) * rec_stride, last);
-            }
+            for (int64_t t = e0 - 1; t >= s0; --t)
+                adjoint_step(h, st, rec + (size_t)(t - s0) * rec_stride, t == seg_start, t,
+                             stage && t >= 1 ? &sp : nullptr, rec_planes);
             CK(cudaEventRecord(ea1, h.stream));
             CK(cudaEventSynchronize(ea1));
             float a1 = 0, a2 = 0;
@@ -1151,16 +1335,69 @@ lbm_status gradient_horizon(lbm_handle& h, const double* w, const lbm_adjoint_op
             CK(cudaEventElapsedTime(&a2, ea0, ea1));
             ms_fwd += a1;
             ms_adj += a2;
+        };
+        auto restore = [&](const Checkpoint& c) {
+            CK(cudaMemcpyAsync(h.pop_array(h.cur), c.buf->p, c.buf->bytes, cudaMemcpyDeviceToDevice, h.stream));
+            h.pending = c.pending;
+            h.t = c.t;
+        };
+        for (int64_t ci = (int64_t)h.ckpts.size() - 1; ci >= 0; --ci) {
+            Checkpoint& c = h.ckpts[ci];
+            const int64_t start = c.t, end = std::min(start + K, T);
+            restore(c);
+            if (end - start <= KR) {
+                reverse_span(start, end, start);
+            } else {
+                // second level: a state every KR steps of the segment
+                std::vector<Checkpoint> sub;
+                cudaEvent_t es0, es1;
+                CK(cudaEventCreate(&es0));
+                CK(cudaEventCreate(&es1));
+                CK(cudaEventRecord(es0, h.stream));
+                const int64_t last = start + ((end - 1 - start) / KR) * KR;  // the last span's first state
+                for (int64_t t = start; t <= last; ++t) {
+                    if ((t - start) % KR == 0) {
+                        Checkpoint sc;
+                        sc.buf = std::make_unique<DevBuf>();
+                        const size_t ab = h.array_bytes(h.storage);
+                        sc.buf->alloc(ab, ctr);
+                        CK(cudaMemcpyAsync(sc.buf->p, h.pop_array(h.cur), ab, cudaMemcpyDeviceToDevice, h.stream));
+                        sc.t = h.t;
+                        sc.pending = h.pending;
+                        sub.push_back(std::move(sc));
+                    }
+                    if (t < last) {
+                        step(h, nullptr, nullptr);
+                        ++recomputed;
+                    }
+                }
+                CK(cudaEventRecord(es1, h.stream));
+                CK(cudaEventSynchronize(es1));
+                float a0 = 0;
+                CK(cudaEventElapsedTime(&a0, es0, es1));
+                ms_fwd += a0;
+                cudaEventDestroy(es0);
+                cudaEventDestroy(es1);
+                int64_t held = 0;
+                for (auto& sc : sub) held += (int64_t)sc.buf->bytes;
+                peak_sub = std::max(peak_sub, held);
+                for (int64_t si = (int64_t)sub.size() - 1; si >= 0; --si) {
+                    restore(sub[si]);
+                    reverse_span(sub[si].t, std::min(sub[si].t + KR, end), start);
+                }
+            }
             // rescale the stored adjoint at segment boundaries
             st.target = next_scale(h, read_norm(h) / st.scale, st.scale);
         }
+        h.peak_extra = peak_sub;
         cudaEventDestroy(ea0);
         cudaEventDestroy(ea1);
     }
     cudaEventDestroy(ef0);
     cudaEventDestroy(ef1);
-    int64_t peak = (int64_t)h.record.bytes;
+    int64_t peak = (int64_t)h.record.bytes + h.peak_extra;
     for (auto& c : h.ckpts) peak += (int64_t)c.buf->bytes;
+    h.peak_extra = 0;
     h.ckpts.clear();
     // the current state is the one of checkpoint 0's segment end; re-mark
     h.forward_done = false;
@@ -1323,7 +1560,7 @@ lbm_status lbm_forward(lbm_handle* h, int64_t steps, lbm_diag_t* diag) {
         h->ckpts.clear();
         init_state(*h);
         const int64_t T = steps > 0 ? steps : h->step_count;
-        lbm_status s = run_admitted(*h, T, diag, 0);
+        lbm_status s = run_admitted(*h, T, diag, 0, h->time_average);
         h->forward_done = true;
         return s;
     });
@@ -1370,7 +1607,7 @@ lbm_status lbm_get_populations(lbm_handle* h, double* f, size_t n) {
         const int Q = h->Q;
         check_n(*h, n, (size_t)(N * Q), "populations");
         ensure_scratch(*h);
-        CK(launch_canon_pop(Q, h->storage, h->G, h->popA(), h->mask.as<uint32_t>(), h->ports_d.as<PortMap>(),
+        CK(launch_canon_pop(Q, h->storage, h->G, h->popA(), h->mask.as<uint32_t>(), ports_at(*h, h->t),
                             h->pending ? 1 : 0, h->scratch.as<float>(), grid_for(*h), h->stream));
         std::vector<float> g((size_t)N * Q);
         CK(cudaMemcpyAsync(g.data(), h->scratch.p, g.size() * 4, cudaMemcpyDeviceToHost, h->stream));
@@ -1402,6 +1639,16 @@ lbm_status lbm_responses(lbm_handle* h, double* out8) {
         if (!h->state_valid) throw StateError("no current state");
         require_design(*h);
         responses(*h, out8, nullptr);
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_time_average(lbm_handle* h, double* out8) {
+    return guarded(h, [&]() {
+        if (!h->time_average) throw ContractError("time averages need a problem created with time_average");
+        if (!h->tavg_valid) throw StateError("no time average: call lbm_forward first");
+        if (!out8) throw ContractError("out8 must not be NULL");
+        for (int k = 0; k < 8; ++k) out8[k] = h->tavg[k];
         return LBM_OK;
     });
 }
@@ -1449,6 +1696,11 @@ lbm_status lbm_gradient(lbm_handle* h, const double* weights, const lbm_adjoint_
             if (!std::isfinite(weights[k])) throw ContractError("response weights must be finite");
         if (o.lambda_storage < LBM_STORE_F32 || o.lambda_storage > LBM_STORE_BF16)
             throw ContractError("lambda_storage must be float32, float16 or bfloat16");
+        if (o.objective != LBM_OBJ_FINAL && o.objective != LBM_OBJ_TIME_AVERAGE)
+            throw ContractError("objective must be final or time_average");
+        if (o.objective == LBM_OBJ_TIME_AVERAGE && (o.mode != LBM_ADJ_HORIZON || !h->time_average))
+            throw ContractError("the time-averaged objective needs the horizon adjoint and a problem created with "
+                                "time_average");
         if (o.mode == LBM_ADJ_STEADY) {
             if (!(o.tolerance > 0)) throw ContractError("steady adjoint tolerance must be positive");
             return gradient_steady(*h, weights, o, grad, report);
@@ -1476,7 +1728,7 @@ lbm_status lbm_step_vjp(lbm_handle* h, const double* state, const double* lambda
             for (int q = 0; q < Q; ++q) v[(size_t)q * N + x] = (float)lambda_next[x * Q + q];
         ensure_scratch(*h);
         CK(cudaMemcpyAsync(h->scratch.p, v.data(), v.size() * 4, cudaMemcpyHostToDevice, h->stream));
-        CK(launch_seed_lam(Q, LBM_STORE_F32, h->G, h->lamA(), h->mask.as<uint32_t>(), h->ports_d.as<PortMap>(),
+        CK(launch_seed_lam(Q, LBM_STORE_F32, h->G, h->lamA(), h->mask.as<uint32_t>(), ports_at(*h, h->t + 1),
                            h->scratch.as<float>(), 1.f, 1, grid_for(*h), h->stream));
         AdjArgs a = adj_args(*h);
         a.record = h->record.as<float>();

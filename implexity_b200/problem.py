@@ -100,6 +100,7 @@ class SolverOptions:
     checkpoint_every: int = 0
     tolerance: float = 1e-8
     max_iterations: int = 100000
+    time_average: bool = False        # also evaluate the responses of every state (stage objective)
 
     @classmethod
     def parse(cls, v: Any) -> "SolverOptions":
@@ -108,9 +109,14 @@ class SolverOptions:
             return o
         if not isinstance(v, dict):
             raise _err("solver_options must be a mapping")
-        known = {"lattice", "collision", "population_storage", "filter", "adjoint"}
+        known = {"lattice", "collision", "population_storage", "filter", "adjoint", "time_average"}
         if set(v) - known:
-            raise _err("solver_options accepts lattice, collision, population_storage, filter and adjoint")
+            raise _err("solver_options accepts lattice, collision, population_storage, filter, adjoint and "
+                       "time_average")
+        ta = v.get("time_average", False)
+        if not isinstance(ta, bool):
+            raise _err("solver_options.time_average must be a boolean")
+        o.time_average = ta
         lat = v.get("lattice", "D3Q19")
         if lat not in ("D3Q19", "D3Q27"):
             raise _err("solver_options.lattice must be D3Q19 or D3Q27")
@@ -226,7 +232,14 @@ class NormalizedProblem:
             for a in range(3):
                 ports[k].velocity_m_s[a] = port["velocity_m_s"][a]
             ports[k].gauge_pressure_Pa = port.get("gauge_pressure_Pa", 0.0)
+            for a in range(3):
+                ports[k].amplitude_m_s[a] = port.get("amplitude_m_s", [0.0, 0.0, 0.0])[a]
+            ports[k].amplitude_Pa = port.get("amplitude_Pa", 0.0)
+            ports[k].frequency_hz = port.get("frequency_hz", 0.0)
+            ports[k].phase_rad = port.get("phase_rad", 0.0)
+            ports[k].ramp_s = port.get("ramp_s", 0.0)
         p.n_ports = len(self.ports)
+        p.time_average = 1 if o.time_average else 0
         p.ports = C.cast(ports, C.POINTER(_abi.Port))
         self._keep = [ports, p]
         return p
@@ -242,7 +255,10 @@ def _ports(value: Any, shape: tuple[int, int, int]) -> list[dict]:
         if kind not in ("velocity", "pressure"):
             raise _err("Port kind must be velocity or pressure")
         required = {"id", "kind", "face", "mask", "velocity_m_s"} | ({"gauge_pressure_Pa"} if kind == "pressure" else set())
-        keys = set(port) - {"reconstruction"}
+        # pulsatile signal (moving/boundary.rs Signal; keys of implexity-physics-fsi problem/fluid.rs:256-322)
+        signal_keys = {"frequency_hz", "phase_rad", "ramp_s"} | (
+            {"amplitude_Pa"} if kind == "pressure" else {"amplitude_m_s"})
+        keys = set(port) - {"reconstruction"} - signal_keys
         pid = port.get("id")
         if keys != required or not isinstance(pid, str) or not pid.strip() or pid in ids:
             raise _err("Unique port id and exact port fields required")
@@ -268,6 +284,22 @@ def _ports(value: Any, shape: tuple[int, int, int]) -> list[dict]:
             if g is None:
                 raise _err("Finite scalar gauge pressure required")
             entry["gauge_pressure_Pa"] = g
+        for key, lo in (("frequency_hz", 0.0), ("phase_rad", None), ("ramp_s", 0.0)):
+            if key in port:
+                val = _scalar(port[key])
+                if val is None or (lo is not None and val < lo):
+                    raise _err(f"Port {key} must be a finite" + (" nonnegative" if lo is not None else "") + " scalar")
+                entry[key] = val
+        if kind == "velocity" and "amplitude_m_s" in port:
+            amp = np.asarray(port["amplitude_m_s"], dtype=float)
+            if amp.shape != (3,) or not np.all(np.isfinite(amp)):
+                raise _err("Port amplitude_m_s requires three finite components")
+            entry["amplitude_m_s"] = [float(x) for x in amp]
+        if kind == "pressure" and "amplitude_Pa" in port:
+            amp_p = _scalar(port["amplitude_Pa"])
+            if amp_p is None:
+                raise _err("Port amplitude_Pa must be a finite scalar")
+            entry["amplitude_Pa"] = amp_p
         out.append(entry)
     return out
 

@@ -189,6 +189,12 @@ class LbmSolver:
         self._check(self.lib.lbm_get_populations(self.h, _dp(out), out.size))
         return out.reshape(self.cells, self.q)
 
+    def time_average(self) -> np.ndarray:
+        """Responses averaged over the states 1..T of the last forward."""
+        out = np.empty(_abi.N_RESPONSES)
+        self._check(self.lib.lbm_time_average(self.h, _dp(out)))
+        return out
+
     def responses(self) -> np.ndarray:
         out = np.empty(_abi.N_RESPONSES)
         self._check(self.lib.lbm_responses(self.h, _dp(out)))
@@ -211,7 +217,12 @@ class LbmSolver:
         tolerance: float = 1e-8,
         max_iterations: int = 100000,
         check_every: int = 50,
+        objective: str = "final",
+        record_budget_bytes: int = 0,
     ) -> tuple[np.ndarray, AdjointReport]:
+        """Design gradient of w . responses: of the final state (objective
+        "final") or of their mean over the horizon's states ("time_average",
+        horizon mode, problems with solver_options.time_average)."""
         w = np.zeros(_abi.N_RESPONSES)
         w[: len(weights)] = np.asarray(weights, dtype=float)
         o = _abi.AdjointOpts()
@@ -221,7 +232,8 @@ class LbmSolver:
         o.max_iterations = int(max_iterations)
         o.check_every = int(check_every)
         o.tolerance = float(tolerance)
-        o.record_budget_bytes = 0
+        o.record_budget_bytes = int(record_budget_bytes)
+        o.objective = {"final": _abi.LBM_OBJ_FINAL, "time_average": _abi.LBM_OBJ_TIME_AVERAGE}[objective]
         grad = np.empty(self.shape)
         rep = _abi.AdjointReport()
         st = self.lib.lbm_gradient(self.h, _dp(w), C.byref(o), _dp(grad), C.byref(rep))

@@ -26,6 +26,8 @@ CONFIGS = {
     "channel48x24x24_trt": ((48, 24, 24), 2000, "trt", None, "uniform"),
     "channel64_trt": ((64, 64, 64), 5000, "trt", None, "uniform"),
 }
+# The unsteady D3Q27 workload: shape, steps, inlet period in steps.
+PULSATILE = {"pulsatile192_d3q27": ((192, 192, 192), 4000, 1000)}
 
 
 def channel_problem(
@@ -102,6 +104,24 @@ def channel_problem(
         "solver_options": opts,
     }
     return problem
+
+
+def pulsatile_problem(shape=(192, 192, 192), steps=4000, lattice="D3Q27", tau=0.8, u_mean=0.04, amp_frac=0.5,
+                      period_steps=1000, ramp_steps=0, storage="float32", box_half_width=1):
+    """The unsteady channel: the plug inlet pulses as u(t) = u_mean (1 + amp_frac
+    sin(2 pi t / (period_steps dt))) (lattice units), optionally ramped in over
+    ramp_steps; the objective is the time average of the responses (solver
+    option time_average)."""
+    prob = channel_problem(shape=shape, steps=steps, tau=tau, u_in=u_mean, collision="trt", lattice=lattice,
+                           storage=storage, box_half_width=box_half_width)
+    dt = prob["step_s"]
+    inlet = prob["ports"][0]
+    inlet["amplitude_m_s"] = [amp_frac * inlet["velocity_m_s"][0], 0.0, 0.0]
+    inlet["frequency_hz"] = 1.0 / (period_steps * dt)
+    inlet["phase_rad"] = 0.0
+    inlet["ramp_s"] = ramp_steps * dt
+    prob["solver_options"]["time_average"] = True
+    return prob
 
 
 def uniform_design(shape, seed=0):

@@ -49,7 +49,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 1
+#define LBM_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define LBM_API __attribute__((visibility("default")))
@@ -113,13 +113,28 @@ enum {
 #define LBM_MAX_PORTS 7
 
 /* One planar port (ports.rs:55-68, normalize_ports :106-272).  Only the
- * default "legacy_moment" reconstruction (ports.rs:343-406) is provided. */
+ * default "legacy_moment" reconstruction (ports.rs:343-406) is provided.
+ *
+ * Pulsatile ports follow the moving engine's port signal
+ * (moving/boundary.rs:98-126, Signal::factors; value at time t,
+ * moving/field.rs:1002-1013): value(t) = ramp(t) * (wave(t) * amplitude +
+ * mean) with wave(t) = sin(2 pi frequency_hz t + phase_rad) (0 when
+ * frequency_hz = 0) and the C2 smoothstep ramp(t) = s^3 (10 - 15 s + 6 s^2),
+ * s = t / ramp_s, for t < ramp_s (1 otherwise or when ramp_s = 0).  The
+ * reconstruction that produces state t uses t = t_index * step_s.  The keys
+ * are those of the reference's port parsing (implexity-physics-fsi/src/
+ * problem/fluid.rs:256-322). */
 typedef struct {
     int32_t kind;             /* lbm_port_kind */
     int32_t face;             /* lbm_face */
     const uint8_t* mask;      /* N booleans, the full-grid port mask */
-    double velocity_m_s[3];
-    double gauge_pressure_Pa; /* pressure ports only */
+    double velocity_m_s[3];   /* mean velocity (tangential only on pressure ports) */
+    double gauge_pressure_Pa; /* pressure ports only: mean gauge pressure */
+    double amplitude_m_s[3];  /* velocity ports: wave amplitude */
+    double amplitude_Pa;      /* pressure ports: wave amplitude */
+    double frequency_hz;      /* >= 0 */
+    double phase_rad;
+    double ramp_s;            /* >= 0 */
 } lbm_port_t;
 
 /* The problem mapping of solver.rs:46-65 after JSON parsing (key sets and
@@ -157,6 +172,10 @@ typedef struct {
     const uint8_t* design_region;  /* N */
     const double* fixed_design;    /* N, in [0,1] */
     const lbm_port_t* ports;       /* n_ports entries */
+    /* nonzero: lbm_forward also evaluates the responses of every state
+     * t = 1..steps (lbm_time_average), and lbm_gradient accepts
+     * LBM_OBJ_TIME_AVERAGE */
+    int32_t time_average;
 } lbm_problem_t;
 
 /* Trajectory admission record (solver.rs:708-793).  Filled by lbm_forward
@@ -185,6 +204,12 @@ typedef struct {
  * (implexity-ad/src/implicit.rs:49-67 semantics). */
 typedef enum { LBM_ADJ_HORIZON = 0, LBM_ADJ_STEADY = 1 } lbm_adjoint_mode;
 
+/* What the weights apply to: the responses of the final state (the
+ * reference's vector of the last state), or their mean over the states
+ * t = 1..steps of the horizon (a stage objective: every state seeds the
+ * adjoint; HORIZON mode, problems created with time_average). */
+typedef enum { LBM_OBJ_FINAL = 0, LBM_OBJ_TIME_AVERAGE = 1 } lbm_objective;
+
 typedef struct {
     int32_t mode;             /* lbm_adjoint_mode */
     int32_t lambda_storage;   /* lbm_storage of the adjoint populations */
@@ -193,6 +218,7 @@ typedef struct {
     int64_t check_every;      /* STEADY: residual readback period */
     double tolerance;         /* STEADY: relative residual */
     int64_t record_budget_bytes; /* HORIZON: device bytes for per-step records (0 = auto) */
+    int32_t objective;        /* lbm_objective */
 } lbm_adjoint_opts_t;
 
 typedef struct {
@@ -272,6 +298,12 @@ LBM_API lbm_status lbm_trajectory(lbm_handle* h, double* mass, double* exchange,
 
 /* The 8 responses of the current state (LBM_R_*), FP64 compensated sums. */
 LBM_API lbm_status lbm_responses(lbm_handle* h, double* out8);
+
+/* The 8 responses averaged over the states t = 1..steps of the last
+ * lbm_forward (problems created with time_average; no reference
+ * counterpart for the LBM problem: the stage objective of the moving
+ * engine's samples, restated). */
+LBM_API lbm_status lbm_time_average(lbm_handle* h, double* out8);
 
 /* Physical fields of the current state (LbmProblem::fields, provider.rs
  * flow_fields): density [N] kg/m^3, velocity [N*3] m/s, gauge pressure [N] Pa.

@@ -145,10 +145,15 @@ bool make_basis(const Lattice& L, Basis& B) {
 struct Port {
     bool pressure = false;
     int axis = 0, sign = 1;
-    double vel[3] = {0, 0, 0};
+    double vel[3] = {0, 0, 0};  // value in force at the current time
     double density = 1.0;
     std::vector<int64_t> cells;
     std::vector<double> jac;  // Q*Q, cell_jacobian at W (ports.rs:512-519)
+    // pulsatile signal (moving/boundary.rs:98-126; value, moving/field.rs:1002-1013)
+    bool pulsatile = false;
+    double mean_vel[3] = {0, 0, 0}, amp_vel[3] = {0, 0, 0};  // lattice units
+    double mean_p = 0, amp_p = 0;                              // Pa
+    double freq = 0, phase = 0, ramp = 0;
 };
 
 struct Row {
@@ -178,8 +183,9 @@ struct orc_problem {
     std::vector<uint8_t> blocked;
     std::vector<uint32_t> source;
     std::vector<uint32_t> readers;  // 2 per slot
-    // ports
-    std::vector<Port> ports;
+    // ports (values follow the port signal: set_port_time)
+    mutable std::vector<Port> ports;
+    double pressure_unit = 1.0;  // 3 / (rho_phys c^2), Pa -> lattice density
     std::vector<int8_t> port_role;  // +1 inlet (velocity), -1 outlet (pressure), 0 otherwise
     int64_t n_inlet = 0, n_outlet = 0;
     // collision
@@ -326,6 +332,47 @@ void reconstruct(const orc_problem& o, const Port& p, const double* f, double* o
 }
 
 // design.rs:282-294
+// Signal::factors (moving/boundary.rs:111-125): C2 smoothstep ramp and the
+// sine wave at time t seconds.
+void signal_factors(const Port& p, double t, double& ramp, double& wave) {
+    ramp = 1.0;
+    if (p.ramp > 0.0 && t < p.ramp) {
+        double s = t / p.ramp;
+        if (s < 0.0) s = 0.0;
+        ramp = s * s * s * (10.0 - s * 15.0 + s * s * 6.0);
+    }
+    wave = p.freq == 0.0 ? 0.0 : std::sin(t * (2.0 * M_PI * p.freq) + p.phase);
+}
+
+// cell_jacobian at W (ports.rs:512-519) for the port's current value.
+void port_jacobian(const orc_problem& o, Port& pt) {
+    const int Q = o.Q;
+    pt.jac.assign(Q * Q, 0.0);
+    double base[27] = {}, pert[27] = {}, r0[27] = {}, r1[27] = {};
+    for (int q = 0; q < Q; ++q) base[q] = o.L.w[q];
+    reconstruct(o, pt, base, r0);
+    for (int kq = 0; kq < Q; ++kq) {
+        for (int q = 0; q < Q; ++q) pert[q] = base[q];
+        pert[kq] += 1.0;
+        reconstruct(o, pt, pert, r1);
+        for (int r = 0; r < Q; ++r) pt.jac[r * Q + kq] = r1[r] - r0[r];
+    }
+}
+
+// Port values of the reconstruction that produces state t_index
+// (t = t_index * dt; moving/field.rs:1002-1013): ramp (wave amplitude + mean).
+void set_port_time(const orc_problem& o, int64_t t_index) {
+    const double t = (double)t_index * o.dt;
+    for (Port& p : o.ports) {
+        if (!p.pulsatile) continue;
+        double ramp, wave;
+        signal_factors(p, t, ramp, wave);
+        if (p.pressure) p.density = 1.0 + ramp * (wave * p.amp_p + p.mean_p) * o.pressure_unit;
+        for (int d = 0; d < 3; ++d) p.vel[d] = ramp * (wave * p.amp_vel[d] + p.mean_vel[d]);
+        port_jacobian(o, p);
+    }
+}
+
 inline double resistance(const orc_problem& o, double phi) {
     return o.dt * o.drag_max * o.drag_shape * (1.0 - phi) / (o.drag_shape + phi);
 }
@@ -1145,6 +1192,7 @@ int orc_create(const lbm_problem_t* p, orc_problem** out) {
     // ports (ports.rs:106-272 normalisation, CompiledPort::new :509-521)
     o->port_role.assign(N, 0);
     double unit = o->dx / o->dt;
+    o->pressure_unit = 3.0 / (o->density * unit * unit);
     for (int k = 0; k < p->n_ports; ++k) {
         const lbm_port_t& src = p->ports[k];
         Port pt;
@@ -1153,18 +1201,19 @@ int orc_create(const lbm_problem_t* p, orc_problem** out) {
         pt.sign = (src.face % 2 == 0) ? 1 : -1;
         for (int d = 0; d < 3; ++d) pt.vel[d] = src.velocity_m_s[d] * o->dt / o->dx;
         if (pt.pressure) pt.density = 1.0 + src.gauge_pressure_Pa * 3.0 / (o->density * unit * unit);
+        for (int d = 0; d < 3; ++d) {
+            pt.mean_vel[d] = pt.vel[d];
+            pt.amp_vel[d] = pt.pressure ? 0.0 : src.amplitude_m_s[d] * o->dt / o->dx;
+        }
+        pt.mean_p = pt.pressure ? src.gauge_pressure_Pa : 0.0;
+        pt.amp_p = pt.pressure ? src.amplitude_Pa : 0.0;
+        pt.freq = src.frequency_hz;
+        pt.phase = src.phase_rad;
+        pt.ramp = src.ramp_s;
+        pt.pulsatile = pt.freq != 0.0 || pt.ramp != 0.0;
         for (int64_t x = 0; x < N; ++x)
             if (src.mask[x]) pt.cells.push_back(x);
-        pt.jac.assign(Q * Q, 0.0);
-        double base[27], pert[27], r0[27], r1[27];
-        for (int q = 0; q < Q; ++q) base[q] = o->L.w[q];
-        reconstruct(*o, pt, base, r0);
-        for (int kq = 0; kq < Q; ++kq) {
-            for (int q = 0; q < Q; ++q) pert[q] = base[q];
-            pert[kq] += 1.0;
-            reconstruct(*o, pt, pert, r1);
-            for (int r = 0; r < Q; ++r) pt.jac[r * Q + kq] = r1[r] - r0[r];
-        }
+        port_jacobian(*o, pt);
         for (int64_t x : pt.cells) o->port_role[x] = pt.pressure ? -1 : 1;
         if (pt.pressure) o->n_outlet += (int64_t)pt.cells.size();
         else o->n_inlet += (int64_t)pt.cells.size();
@@ -1238,6 +1287,7 @@ void orc_history_trace(const orc_problem* o, const double* alpha, int64_t steps,
         mach = std::max(mach, wv);
         finite = finite && fin;
         if (t == steps) break;
+        set_port_time(*o, t + 1);
         changes[t] = interval(*o, a.data(), alpha, b.data(), post);
         std::swap(a, b);
     }
@@ -1279,6 +1329,8 @@ void orc_interval_vjp(const orc_problem* o, const double* before, const double* 
     interval_vjp(*o, before, alpha, after_bar, f_bar, alpha_bar);
 }
 
+void orc_set_time(const orc_problem* o, int64_t t_index) { set_port_time(*o, t_index); }
+
 void orc_port_apply(const orc_problem* o, int port, const double* f_in, double* f_out) {
     reconstruct(*o, o->ports[port], f_in, f_out);
 }
@@ -1300,19 +1352,31 @@ int orc_gradient(const orc_problem* o, const double* raw, const double* w8, int6
     initial(*o, x.data());
     ckpt.push_back({0, x});
     int64_t evals = 0;
+    // mode 2: the weighted responses averaged over the states 1..steps (a
+    // stage objective: every state seeds the adjoint with weights w/steps)
+    const bool stage = mode == 2;
+    double ws[8], avg[8] = {0, 0, 0, 0, 0, 0, 0, 0}, r8[8];
+    for (int k = 0; k < 8; ++k) ws[k] = stage ? w8[k] / (double)steps : w8[k];
     for (int64_t t = 0; t < steps; ++t) {
+        set_port_time(*o, t + 1);
         interval(*o, x.data(), alpha.data(), nx.data(), post);
         ++evals;
         std::swap(x, nx);
         if ((t + 1) % K == 0 && t + 1 < steps) ckpt.push_back({t + 1, x});
+        if (stage) {
+            vector(*o, phi.data(), alpha.data(), x.data(), r8);
+            for (int k = 0; k < 8; ++k) avg[k] += r8[k] / (double)steps;
+        }
     }
-    vector(*o, phi.data(), alpha.data(), x.data(), responses8);
+    if (stage) std::memcpy(responses8, avg, sizeof(avg));
+    else vector(*o, phi.data(), alpha.data(), x.data(), responses8);
     std::vector<double> lam(NQ), abar_final(N), phibar(N), abar(N, 0.0), fb(NQ), ab(N);
-    vector_vjp(*o, phi.data(), alpha.data(), x.data(), w8, lam.data(), abar_final.data(), phibar.data());
+    vector_vjp(*o, phi.data(), alpha.data(), x.data(), ws, lam.data(), abar_final.data(), phibar.data());
+    std::vector<double> sf(NQ), sa(N), sp(N);
     int status = 0;
     int64_t iters = 0;
     double resid = 0;
-    if (mode == 0) {
+    if (mode == 0 || mode == 2) {
         while (!ckpt.empty()) {
             auto [start, xs] = std::move(ckpt.back());
             ckpt.pop_back();
@@ -1321,15 +1385,27 @@ int orc_gradient(const orc_problem* o, const double* raw, const double* w8, int6
             states.push_back(std::move(xs));
             for (int64_t t = start; t + 1 < end; ++t) {
                 std::vector<double> nxt(NQ);
+                set_port_time(*o, t + 1);
                 interval(*o, states.back().data(), alpha.data(), nxt.data(), post);
                 ++evals;
                 states.push_back(std::move(nxt));
             }
             for (int64_t t = end - 1; t >= start; --t) {
+                set_port_time(*o, t + 1);
                 interval_vjp(*o, states[t - start].data(), alpha.data(), lam.data(), fb.data(), ab.data());
                 for (int64_t c = 0; c < N; ++c) abar[c] += ab[c];
                 std::swap(lam, fb);
                 ++iters;
+                if (stage && t >= 1) {
+                    // the stage seed of state t
+                    vector_vjp(*o, phi.data(), alpha.data(), states[t - start].data(), ws, sf.data(), sa.data(),
+                               sp.data());
+                    for (int64_t i = 0; i < NQ; ++i) lam[i] += sf[i];
+                    for (int64_t c = 0; c < N; ++c) {
+                        abar[c] += sa[c];
+                        phibar[c] += sp[c];
+                    }
+                }
             }
         }
     } else {
@@ -1338,6 +1414,7 @@ int orc_gradient(const orc_problem* o, const double* raw, const double* w8, int6
             for (double e : v) s += e * e;
             return std::sqrt(s);
         };
+        set_port_time(*o, steps);
         double n0 = norm(lam);
         status = 2;
         if (n0 == 0) status = 0;

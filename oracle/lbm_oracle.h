@@ -81,7 +81,10 @@ void orc_interval_vjp(const orc_problem* o, const double* before, const double* 
 
 /* provider.rs:332-365 chain.  mode 0: fixed horizon with scan Every(K)
  * checkpoints (K <= 0: all states kept); mode 1: steady Neumann series at the
- * final state until |lambda_k| <= tol |lambda_0| or max_iter.
+ * final state until |lambda_k| <= tol |lambda_0| or max_iter; mode 2: the
+ * fixed horizon for the weighted responses averaged over states 1..steps
+ * (responses8 returns the averages).  Pulsatile ports take their values at
+ * the time of the state each reconstruction produces.
  * Returns 0 on success, 2 if the steady iteration did not converge. */
 typedef struct {
     int64_t iterations;
@@ -95,6 +98,10 @@ int orc_gradient(const orc_problem* o, const double* raw, const double* w8, int6
 /* MRT moment basis (collision.rs:87-153): rows[Q*Q], norms[Q], groups[Q]
  * (0 mass, 1 momentum, 2 bulk, 3 shear, 4 odd, 5 even-high) */
 int orc_mrt_basis(int q, double* rows, double* norms, int32_t* groups);
+
+/* Sets the port values (pulsatile signals) to those of the reconstruction
+ * producing state t_index; orc_interval / orc_interval_vjp then use them. */
+void orc_set_time(const orc_problem* o, int64_t t_index);
 
 /* Port reconstruction of one cell (ports.rs:343-406) for port index k. */
 void orc_port_apply(const orc_problem* o, int port, const double* f_in, double* f_out);

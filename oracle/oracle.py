@@ -82,6 +82,8 @@ def lib() -> C.CDLL:
         L.orc_gradient.argtypes = [h, _dp, _dp, C.c_int64, C.c_int, C.c_int64, C.c_double, C.c_int64, _dp, _dp,
                                    C.POINTER(GradReport)]
         L.orc_mrt_basis.argtypes = [C.c_int, _dp, _dp, C.POINTER(C.c_int32)]
+        L.orc_set_time.argtypes = [h, C.c_int64]
+        L.orc_set_time.restype = None
         L.orc_port_apply.argtypes = [h, C.c_int, _dp, _dp]
         L.orc_port_apply.restype = None
         _lib = L
@@ -211,9 +213,14 @@ class Oracle:
         resp = np.empty(8)
         rep = GradReport()
         steps = self.problem.step_count if steps is None else steps
-        st = lib().orc_gradient(self.h, _p(raw), _p(w8), int(steps), 1 if mode == "steady" else 0, int(K),
+        m = {"horizon": 0, "steady": 1, "time_average": 2}[mode]
+        st = lib().orc_gradient(self.h, _p(raw), _p(w8), int(steps), m, int(K),
                                 float(tol), int(max_iter), _p(grad), _p(resp), C.byref(rep))
         return grad, resp, rep, st
+
+    def set_time(self, t_index: int):
+        """Port values of the reconstruction producing state t_index."""
+        lib().orc_set_time(self.h, int(t_index))
 
     def port_apply(self, k, f):
         f = np.ascontiguousarray(f, dtype=np.float64)
