@@ -30,6 +30,7 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
     constexpr int NREC = STG ? 10 : 4;
     using S = AdjStage<Q, T, NREC>;
     constexpr int NCOPY = Q + NREC + 2;  // runs of lambda, the record, mask and alpha
+    constexpr int STAGES = Ring<T>::STAGES;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);  // stage loaded
     uint64_t* empty = full + STAGES;                      // stage consumed
@@ -82,9 +83,12 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
         int s = 0;
         uint32_t round = 0;
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            const uint32_t x = tile * TILE + c;
+            // the running alpha cotangent, read before the wait so that its
+            // latency hides behind the staged copies and the collision
+            const float ab_prev = (!a.overwrite_abar && x < n) ? a.abar[x] : 0.f;
             const bool ok = mbar_wait(&full[s], round & 1u, a.err);
             const S* st = stage_at<S>(smem, s);
-            const uint32_t x = tile * TILE + c;
             const uint32_t m = ok && x < n ? st->mask[c] : MASK_SOLID;
             const bool fluid = !(m & MASK_SOLID);
             float v[Q];
@@ -123,8 +127,7 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
                         for (int q = 0; q < Q; ++q) v[q] += fb[q];
                     }
                 }
-                if (a.overwrite_abar) a.abar[x] = ab * a.abar_factor;
-                else a.abar[x] = fmaf(ab, a.abar_factor, a.abar[x]);
+                a.abar[x] = fmaf(ab, a.abar_factor, ab_prev);
                 if (a.port_transpose && (m & MASK_PORT)) port_transpose<Q>(a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], v);
                 store_own_lam<Q, T>(D, n, x, v, a.out_scale);
                 if (a.norm2) {
@@ -153,7 +156,7 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
 
 template <int Q, int COLL, typename T, int AL, int STG>
 cudaError_t run_adjoint_al(const AdjArgs& a, cudaStream_t s) {
-    constexpr size_t smem = pipe_bytes<AdjStage<Q, T, STG ? 10 : 4>>();
+    constexpr size_t smem = pipe_bytes<AdjStage<Q, T, STG ? 10 : 4>, Ring<T>::STAGES>();
     static bool attr = false;
     if (!attr) {
         cudaError_t e = set_smem(k_adjoint<Q, COLL, T, AL, STG>, smem);

@@ -658,6 +658,41 @@ __device__ __forceinline__ float response_vjp(float rp, const float (&u)[3], con
     return abar;
 }
 
+// Integrands of the responses of one fluid cell (vector_cell, solver.rs:
+// 835-895, plus the viscous dissipation of response_vjp), in FP32 from the
+// cell's moments: out = {U_x, U_y, U_z, R |U|^2, R alpha |U|^2 / dt,
+// sigma:sigma / (2 rho nu)} in the units that sums_to_responses scales.  The
+// design density and the pressure drop are added by the caller.
+template <int Q>
+__device__ __forceinline__ void response_cell(float rp, const float (&u)[3], const float (&S)[6], float alpha,
+                                              const SeedParams& sp, const Physics& P, float (&out)[6]) {
+    const float k = 1.f - 0.5f / sp.tau;
+    const float nu = (sp.tau - 0.5f) / 3.f;
+    const float rho = 1.f + rp;
+    float F[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) F[d] = rho * (P.a[d] - alpha * u[d]);
+    const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+    float ss = 0.f;
+#pragma unroll
+    for (int e = 0; e < 6; ++e) {
+        const float pi = S[e] - (e < 3 ? rp / 3.f : 0.f) - rho * u[ia[e]] * u[ib[e]];
+        const float t = 0.5f * (u[ia[e]] * F[ib[e]] + u[ib[e]] * F[ia[e]]);
+        const float sg = -k * (pi + t);
+        ss += (e < 3 ? 1.f : 2.f) * sg * sg;
+    }
+    const float V = sp.vel;
+    const float U[3] = {u[0] * V, u[1] * V, u[2] * V};
+    const float usq = U[0] * U[0] + U[1] * U[1] + U[2] * U[2];
+    const float R = rho * sp.dens;
+    out[0] = U[0];
+    out[1] = U[1];
+    out[2] = U[2];
+    out[3] = R * usq;
+    out[4] = R * alpha / sp.dt_s * usq;
+    out[5] = ss / (2.f * rho * nu);
+}
+
 // ------------------------------------------------------------------ reductions
 __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
     s = a + b;
@@ -945,7 +980,20 @@ namespace {
 constexpr int CONSUMER_WARPS = 8;
 constexpr int TILE = CONSUMER_WARPS * 32;
 constexpr int TPB = CONSUMER_WARPS * 32 + 32;
-constexpr int STAGES = 3;
+// Ring depth per storage width: a 16-bit tile carries half the bytes of a
+// 32-bit one, so more of them are kept in flight for the same bytes.
+#ifndef LBM_STAGES_32
+#define LBM_STAGES_32 3
+#endif
+#ifndef LBM_STAGES_16
+#define LBM_STAGES_16 3
+#endif
+template <typename T>
+struct Ring {
+    static constexpr int STAGES = sizeof(T) == 4 ? LBM_STAGES_32 : LBM_STAGES_16;
+    static_assert(STAGES >= 2 && STAGES <= 10, "ring depth");
+};
+constexpr int PIPE_HEAD = 256;  // full/empty/rdone mbarriers of up to 10 stages
 
 template <typename T>
 struct Vec16 {
@@ -960,13 +1008,13 @@ template <typename S>
 __host__ __device__ constexpr size_t stage_stride() {
     return (sizeof(S) + 127) / 128 * 128;
 }
-template <typename S>
+template <typename S, int NS>
 __host__ __device__ constexpr size_t pipe_bytes() {
-    return 128 + STAGES * stage_stride<S>();
+    return PIPE_HEAD + NS * stage_stride<S>();
 }
 template <typename S>
 __device__ __forceinline__ S* stage_at(unsigned char* smem, int s) {
-    return reinterpret_cast<S*>(smem + 128 + s * stage_stride<S>());
+    return reinterpret_cast<S*>(smem + PIPE_HEAD + s * stage_stride<S>());
 }
 
 // Misalignment of direction q's staged run when the plane stride n and the

@@ -22,10 +22,13 @@ struct FwdStage {
     float alpha[FRUN];
 };
 
-template <int Q, int COLL, typename T, int AL>
+// RSP = 1: the step also sums the responses of the state it reads (the
+// stage objective's per-state values; vector_cell, solver.rs:835-895).
+template <int Q, int COLL, typename T, int AL, int RSP>
 __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
     using L = Lat<Q>;
     using S = FwdStage<Q, T>;
+    constexpr int STAGES = Ring<T>::STAGES;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);  // stage loaded
     uint64_t* empty = full + STAGES;                      // stage consumed (outputs written into it)
@@ -42,6 +45,7 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
     const bool bulk_ok = a.collide && a.bulk_store;
     DiagLocal acc;
     acc.init();
+    double rsum[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // per-thread response sums (RSP)
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int s = 0; s < STAGES; ++s) {
@@ -103,6 +107,9 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
             float v[Q];
             const uint32_t m = ok && x < n ? st->mask[c] : MASK_SOLID;
             const bool fluid = !(m & MASK_SOLID);
+            if constexpr (RSP) {
+                if (!fluid && ok && x < n) rsum[5] += (double)a.phi[x];
+            }
             if (fluid) {
                 if (!(m & MASK_WRAP)) {
 #pragma unroll
@@ -137,16 +144,31 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
                     }
                 }
                 const float mn = a.diag ? min_population<Q, SC>(v) : 0.f;
-                if (a.record && a.record_s) {
-                    // second moments of g for the stage seeds of the adjoint
-                    float g[Q], S[6];
+                float S[6];
+                if (RSP || (a.record && a.record_s)) {
+                    // second moments of g: the stage seeds of the adjoint, the dissipation
+                    float g[Q];
 #pragma unroll
                     for (int q = 0; q < Q; ++q) g[q] = SC ? L::w(q) * v[q] : v[q];
                     second_moments<Q>(g, S);
+                    if (a.record && a.record_s) {
 #pragma unroll
-                    for (int e = 0; e < 6; ++e) a.record[(size_t)(4 + e) * n + x] = S[e];
+                        for (int e = 0; e < 6; ++e) a.record[(size_t)(4 + e) * n + x] = S[e];
+                    }
                 }
                 const Macro M = collide_fused<Q, COLL, SC>(v, alpha, a.P, a.collide);
+                if constexpr (RSP) {
+                    float r6[6];
+                    response_cell<Q>(M.rp, M.u, S, alpha, a.sp, a.P, r6);
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) rsum[k] += (double)r6[k];
+                    rsum[5] += (double)a.phi[x];
+                    if (m & MASK_PORT) {
+                        const float dpw = a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1].dp_weight;
+                        rsum[6] += (double)(dpw * a.sp.dens * M.rp * a.sp.vel * a.sp.vel / 3.f);
+                    }
+                    rsum[7] += (double)r6[5];
+                }
                 if (a.diag) {
                     acc.mass += M.rp;
                     acc.exch += exch;
@@ -188,20 +210,34 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
         }
     }
     if (a.diag) finish_diag(acc, a.diag, a.red);
+    if constexpr (RSP) {
+        Sums<8> t;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            t.h[k] = rsum[k];
+            t.l[k] = 0.0;
+        }
+        finish_sums<8>(t, a.stage, a.red2);
+    }
+}
+
+template <int Q, int COLL, typename T, int AL, int RSP>
+cudaError_t run_forward_rs(const FwdArgs& a, cudaStream_t s) {
+    constexpr size_t smem = pipe_bytes<FwdStage<Q, T>, Ring<T>::STAGES>();
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = set_smem(k_forward<Q, COLL, T, AL, RSP>, smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const int grid = persistent_grid((const void*)k_forward<Q, COLL, T, AL, RSP>, a.G.n, smem, TPB, TILE);
+    k_forward<Q, COLL, T, AL, RSP><<<grid, TPB, smem, s>>>(a);
+    return cudaGetLastError();
 }
 
 template <int Q, int COLL, typename T, int AL>
 cudaError_t run_forward_al(const FwdArgs& a, cudaStream_t s) {
-    constexpr size_t smem = pipe_bytes<FwdStage<Q, T>>();
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = set_smem(k_forward<Q, COLL, T, AL>, smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
-    const int grid = persistent_grid((const void*)k_forward<Q, COLL, T, AL>, a.G.n, smem, TPB, TILE);
-    k_forward<Q, COLL, T, AL><<<grid, TPB, smem, s>>>(a);
-    return cudaGetLastError();
+    return a.stage ? run_forward_rs<Q, COLL, T, AL, 1>(a, s) : run_forward_rs<Q, COLL, T, AL, 0>(a, s);
 }
 
 // The run offsets are compile-time constants when every run table entry

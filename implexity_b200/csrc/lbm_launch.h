@@ -36,6 +36,12 @@ struct FwdArgs {
     int32_t bulk_store;      // full tiles leave through bulk stores (planes 16-byte aligned)
     uint32_t step;           // absolute step index (seeds the stochastic rounding)
     int* err;                // set when a bounded wait gave up
+    // response sums of the state the step reads (16 doubles: 8 compensated
+    // sums; nullptr: off), with their own reduction scratch
+    double* stage;
+    Reduce red2;
+    const float* phi;        // design density (response 5)
+    SeedParams sp;           // unit conversions of the responses (w unused)
     // staged pull runs: element offset of each direction's 16-byte aligned
     // run for the tile at x0 = 0, and the offset of the tile's first element
     // inside it

@@ -736,7 +736,7 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
     h.offsets_d.alloc(std::max<size_t>(1, h.offsets.size()) * sizeof(int4), ctr);
     h.ports_d.alloc(std::max<size_t>(1, maps.size()) * sizeof(PortMap), ctr);
     h.partial.alloc((size_t)h.sms * 32 * 16 * sizeof(double), ctr);
-    h.counter.alloc(sizeof(unsigned), ctr);
+    h.counter.alloc(2 * sizeof(unsigned), ctr);  // [0] step/objective sums, [1] fused response sums
     h.sums.alloc(64 * sizeof(double), ctr);
     CK(cudaMemsetAsync(h.mask.p, 0xff, (size_t)(n + CELL_PAD) * 4, h.stream));  // padding reads as solid
     CK(cudaMemcpyAsync(h.mask.p, mask.data(), (size_t)n * 4, cudaMemcpyHostToDevice, h.stream));
@@ -749,7 +749,7 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
     if (!maps.empty())
         CK(cudaMemcpyAsync(h.ports_d.p, maps.data(), maps.size() * sizeof(PortMap), cudaMemcpyHostToDevice,
                            h.stream));
-    CK(cudaMemsetAsync(h.counter.p, 0, sizeof(unsigned), h.stream));
+    CK(cudaMemsetAsync(h.counter.p, 0, 2 * sizeof(unsigned), h.stream));
     CK(cudaMemsetAsync(h.errflag.p, 0, sizeof(int), h.stream));
     CK(cudaMemsetAsync(h.pop.p, 0, h.pop.bytes, h.stream));
     CK(cudaStreamSynchronize(h.stream));
@@ -778,14 +778,23 @@ FwdArgs fwd_args(lbm_handle& h) {
     a.ports = ports_at(h, h.t);
     a.red = reduce_of(h);
     a.err = h.errflag.as<int>();
+    // the fused response sums reduce through the upper half of the scratch
+    a.red2 = Reduce{h.partial.as<double>() + (size_t)h.sms * 32 * 8, h.counter.as<unsigned>() + 1};
+    a.phi = h.phi.as<float>();
+    a.sp.vel = (float)(h.dx / h.dt);
+    a.sp.dens = (float)h.density;
+    a.sp.dt_s = (float)h.dt;
+    a.sp.tau = (float)h.tau;
     return a;
 }
 
 int coll_kind(const lbm_handle& h) { return h.coll == LBM_MRT ? CK_MRT : CK_PAIRS; }
 
-// One step of the current state; diag / record optional.
-void step(lbm_handle& h, StepDiag* diag, float* record, bool record_s = false) {
+// One step of the current state; diag / record / the current state's
+// response sums (16 doubles) optional.
+void step(lbm_handle& h, StepDiag* diag, float* record, bool record_s = false, double* stage = nullptr) {
     FwdArgs a = fwd_args(h);
+    a.stage = stage;
     a.apply_ports = h.pending ? 1 : 0;
     a.diag = diag;
     a.record = record;
@@ -799,8 +808,9 @@ void step(lbm_handle& h, StepDiag* diag, float* record, bool record_s = false) {
 }
 
 // Load-only pass of the current state (admission reductions and/or record).
-void inspect(lbm_handle& h, StepDiag* diag, float* record, bool record_s = false) {
+void inspect(lbm_handle& h, StepDiag* diag, float* record, bool record_s = false, double* stage = nullptr) {
     FwdArgs a = fwd_args(h);
+    a.stage = stage;
     a.dst = nullptr;
     a.apply_ports = h.pending ? 1 : 0;
     a.diag = diag;
@@ -891,11 +901,12 @@ void check_errflag(lbm_handle& h) {
 
 // Runs `steps` steps from the current state with admission of every state
 // including the current one.  Optionally stores checkpoints every K steps.
-void stage_sums(lbm_handle& h, double* slot);
 void finish_time_average(lbm_handle& h, int64_t steps);
 
 // With `averages`, the responses of every state 1..steps are summed on the
-// device as well (the stage objective's value, lbm_time_average).
+// device as well (the stage objective's value, lbm_time_average): the step
+// that reads state t sums its responses into slot t, the final inspection
+// those of the last state.
 lbm_status run_admitted(lbm_handle& h, int64_t steps, lbm_diag_t* out, int64_t K, bool averages = false) {
     require_design(h);
     int64_t* ctr = &h.device_bytes;
@@ -917,10 +928,10 @@ lbm_status run_admitted(lbm_handle& h, int64_t steps, lbm_diag_t* out, int64_t K
             c.pending = h.pending;
             h.ckpts.push_back(std::move(c));
         }
-        step(h, d + s, nullptr);
-        if (averages) stage_sums(h, h.tsums.as<double>() + (size_t)(s + 1) * 16);
+        double* slot = averages && s > 0 ? h.tsums.as<double>() + (size_t)s * 16 : nullptr;
+        step(h, d + s, nullptr, false, slot);
     }
-    inspect(h, d + steps, nullptr);
+    inspect(h, d + steps, nullptr, false, averages ? h.tsums.as<double>() + (size_t)steps * 16 : nullptr);
     CK(cudaEventRecord(h.ev1, h.stream));
     std::vector<StepDiag>& hd = h.last_trajectory;
     hd.resize((size_t)steps + 1);
@@ -981,14 +992,7 @@ void responses(lbm_handle& h, double* out8, float* fields) {
     sums_to_responses(h, s, out8);
 }
 
-// Responses of the current state, summed into a device slot (16 doubles).
-void stage_sums(lbm_handle& h, double* slot) {
-    ObjArgs a = obj_args(h);
-    a.sums = slot;
-    CK(launch_objective(h.Q, h.storage, LBM_STORE_F32, 0, a, grid_for(h), h.stream));
-}
-
-// Mean of the responses of states 1..steps (slots filled by stage_sums).
+// Mean of the responses of states 1..steps (slots filled by the steps).
 void finish_time_average(lbm_handle& h, int64_t steps) {
     std::vector<double> all((size_t)(steps + 1) * 16);
     CK(cudaMemcpy(all.data(), h.tsums.p, all.size() * sizeof(double), cudaMemcpyDeviceToHost));

@@ -2,17 +2,21 @@
 // completed through an mbarrier, for the staged tiles of the stepping
 // kernels.  sm_90+ PTX; the kernels here are compiled for sm_100a only.
 //
-// Every wait is bounded: after kWaitLimit polls the waiting thread records
-// the failure in a device flag (the host turns it into LBM_E_CUDA) and keeps
-// waiting for a second bounded period so that no copy is left in flight into
-// shared memory when the block exits.
+// Every wait is bounded in time: after kWaitNs of the global timer the
+// waiting thread records the failure in a device flag (the host turns it into
+// LBM_E_CUDA) and keeps waiting for a second bounded period so that no copy is
+// left in flight into shared memory when the block exits.  Each poll asks the
+// hardware to suspend the thread until the phase completes (suspend-time
+// hint), so waiting warps leave the issue slots to the computing ones instead
+// of spinning.
 #pragma once
 
 #include <cstdint>
 
 namespace lbm {
 
-constexpr uint32_t kWaitLimit = 1u << 24;
+constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s per bounded period
+constexpr uint32_t kSuspendHintNs = 10000000u;  // per poll; the thread wakes when the phase completes
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -41,22 +45,35 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendHintNs)
         : "memory");
     return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Polls until the phase completes or kWaitNs have passed since t0.
+__device__ __forceinline__ bool mbar_poll_until(uint64_t* bar, uint32_t parity, uint64_t t0) {
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > kWaitNs) return false;
+    }
 }
 
 // Bounded wait for the phase with the given parity.  Returns false (and sets
 // *err) if the copies did not land within the limit.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-    for (uint32_t i = 0; i < kWaitLimit; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_poll_until(bar, parity, global_ns())) return true;
     if (err) atomicOr(err, 1);
-    for (uint32_t i = 0; i < kWaitLimit; ++i)
-        if (mbar_try_wait(bar, parity)) break;
+    mbar_poll_until(bar, parity, global_ns());
     return false;
 }
 

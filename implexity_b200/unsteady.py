@@ -3,7 +3,8 @@ checkpointed adjoint for several checkpoint intervals K.
 
 D3Q27 TRT channel with a pulsatile plug inlet u(t) = 0.04 (1 + 0.5 sin(2 pi t /
 (1000 dt))) (lattice units), 4000 steps, objective = the time average of the
-pressure drop + viscous dissipation over the states 1..T.  The adjoint is the
+viscous dissipation (or the weighted responses of the channel objective)
+over the states 1..T.  The adjoint is the
 horizon adjoint with a checkpoint every K steps (scan.rs Every(K)); when a
 segment's per-step records do not fit in device memory, each segment is split
 once more (a second checkpoint level).  For every K the report gives the
@@ -27,12 +28,21 @@ from .problem import normalize
 from .solver import LbmSolver
 
 
-def run(shape, steps, Ks, period_steps=1000, storage="float32", seed=0, log=print):
+def weights(objective: str) -> np.ndarray:
+    """'dissipation': response 7 alone; 'channel': pressure drop + dissipation."""
+    if objective == "dissipation":
+        w = np.zeros(8)
+        w[7] = 1.0
+        return w
+    return workloads.objective_weights()
+
+
+def run(shape, steps, Ks, period_steps=1000, storage="float32", seed=0, objective="dissipation", log=print):
     prob = workloads.pulsatile_problem(shape=tuple(shape), steps=steps, lattice="D3Q27", period_steps=period_steps,
                                        storage=storage)
     norm = normalize(prob)
     raw = workloads.uniform_design(tuple(shape), seed)
-    w = workloads.objective_weights()
+    w = weights(objective)
     out = []
     with LbmSolver(norm) as s:
         s.set_design(raw)
@@ -42,6 +52,7 @@ def run(shape, steps, Ks, period_steps=1000, storage="float32", seed=0, log=prin
         avg = s.time_average()
         j = float(np.dot(w, avg))
         base = {"workload": "pulsatile_d3q27", "shape": list(shape), "steps": steps, "storage": storage,
+                "objective": objective,
                 "objective_time_average": j, "forward_ms": d.device_ms, "forward_wall_s": fwd_wall,
                 "forward_mlups": s.cells * steps / (d.device_ms / 1e3) / 1e6}
         log(json.dumps(base))
@@ -69,8 +80,9 @@ def main():
     ap.add_argument("--K", type=int, nargs="+", default=[50, 200, 800])
     ap.add_argument("--period-steps", type=int, default=1000)
     ap.add_argument("--storage", choices=["float32", "float16"], default="float32")
+    ap.add_argument("--objective", choices=["dissipation", "channel"], default="dissipation")
     a = ap.parse_args()
-    run(a.shape, a.steps, a.K, a.period_steps, a.storage)
+    run(a.shape, a.steps, a.K, a.period_steps, a.storage, objective=a.objective)
 
 
 if __name__ == "__main__":
