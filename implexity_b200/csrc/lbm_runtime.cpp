@@ -1291,7 +1291,10 @@ lbm_status gradient_horizon(lbm_handle& h, const double* w, const lbm_adjoint_op
         if (o.record_budget_bytes > 0) budget = std::min(budget, (double)o.record_budget_bytes);
         const int64_t fit = budget > 0 ? (int64_t)(budget / (double)rec_bytes) : 0;
         if (fit < 1) throw ContractError("checkpoint interval needs more record memory than record_budget_bytes");
-        KR = std::min(K, fit);
+        // the fewest spans, of equal length: the same recomputation as the
+        // longest spans that fit, with less record memory
+        const int64_t spans = (K + fit - 1) / fit;
+        KR = (K + spans - 1) / spans;
     }
     h.record.alloc(rec_bytes * (size_t)KR + CELL_PAD * sizeof(float), ctr);
     h.ckpts.clear();
