@@ -9,7 +9,7 @@ import ctypes as C
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "liblbm_b200.so"
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 # status codes
 LBM_OK, LBM_E_CONTRACT, LBM_E_CONVERGENCE, LBM_E_CUDA, LBM_E_STATE = 0, 1, 2, 3, 4
@@ -22,6 +22,7 @@ FACES = ["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"]
 LBM_FILTER_CONIC, LBM_FILTER_BOX = 0, 1
 LBM_ADJ_HORIZON, LBM_ADJ_STEADY = 0, 1
 LBM_OBJ_FINAL, LBM_OBJ_TIME_AVERAGE = 0, 1
+LBM_CKPT_EVERY, LBM_CKPT_BINOMIAL = 0, 1
 N_RESPONSES = 8
 MAX_PORTS = 7
 
@@ -40,6 +41,7 @@ EXPORTS = [
     "lbm_trajectory",
     "lbm_responses",
     "lbm_time_average",
+    "lbm_binomial_plan",
     "lbm_fields",
     "lbm_gradient",
     "lbm_step_vjp",
@@ -121,6 +123,8 @@ class AdjointOpts(C.Structure):
         ("tolerance", C.c_double),
         ("record_budget_bytes", C.c_int64),
         ("objective", C.c_int32),
+        ("checkpointing", C.c_int32),
+        ("snapshots", C.c_int64),
     ]
 
 
@@ -171,6 +175,7 @@ def _declare(lib: C.CDLL) -> None:
     lib.lbm_trajectory.argtypes = [h, _dp, _dp, _dp, _dp, C.c_size_t]
     lib.lbm_responses.argtypes = [h, _dp]
     lib.lbm_time_average.argtypes = [h, _dp]
+    lib.lbm_binomial_plan.argtypes = [C.c_int64, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.lbm_fields.argtypes = [h, _dp, _dp, _dp]
     lib.lbm_gradient.argtypes = [h, _dp, C.POINTER(AdjointOpts), _dp, C.POINTER(AdjointReport)]
     lib.lbm_step_vjp.argtypes = [h, _dp, _dp, _dp, _dp, C.c_size_t]

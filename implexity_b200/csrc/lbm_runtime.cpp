@@ -18,6 +18,7 @@
 #include "../../include/lbm_b200.h"
 #include "lbm_common.cuh"
 #include "lbm_launch.h"
+#include "lbm_revolve.h"
 
 using namespace lbm;
 
@@ -287,6 +288,11 @@ struct DevBuf {
         }
         p = nullptr;
         bytes = 0;
+    }
+    // exactly b bytes (releases a larger buffer)
+    void fit(size_t b, int64_t* ctr) {
+        if (p && bytes != b) reset();
+        alloc(b, ctr);
     }
     void alloc(size_t b, int64_t* ctr) {
         if (p && bytes >= b) return;
@@ -1282,6 +1288,7 @@ lbm_status gradient_horizon(lbm_handle& h, const double* w, const lbm_adjoint_op
     // KR steps, then each span once more with its records (scan.rs Every(K)
     // nested in itself; one more recomputed forward).
     int64_t KR = K;
+    h.record.reset();  // sized below from the memory left
     {
         size_t free_b = 0, total_b = 0;
         CK(cudaMemGetInfo(&free_b, &total_b));
@@ -1296,7 +1303,7 @@ lbm_status gradient_horizon(lbm_handle& h, const double* w, const lbm_adjoint_op
         const int64_t spans = (K + fit - 1) / fit;
         KR = (K + spans - 1) / spans;
     }
-    h.record.alloc(rec_bytes * (size_t)KR + CELL_PAD * sizeof(float), ctr);
+    h.record.fit(rec_bytes * (size_t)KR + CELL_PAD * sizeof(float), ctr);
     h.ckpts.clear();
     // forward with checkpoints, then admission (the reference re-runs parts())
     init_state(h);
@@ -1407,6 +1414,179 @@ lbm_status gradient_horizon(lbm_handle& h, const double* w, const lbm_adjoint_op
     h.peak_extra = 0;
     h.ckpts.clear();
     // the current state is the one of checkpoint 0's segment end; re-mark
+    h.forward_done = false;
+    h.state_valid = false;
+    check_errflag(h);
+    cudaEvent_t e4;
+    CK(cudaEventCreate(&e4));
+    CK(cudaEventRecord(e4, h.stream));
+    finish_gradient(h, st, st.steps > 0, grad);
+    float ms_sens = 0;
+    CK(cudaEventRecord(h.ev1, h.stream));
+    CK(cudaEventSynchronize(h.ev1));
+    CK(cudaEventElapsedTime(&ms_sens, e4, h.ev1));
+    cudaEventDestroy(e4);
+    if (rep) {
+        rep->residual = 0;
+        rep->iterations = st.steps;
+        rep->forward_recomputed = recomputed;
+        rep->peak_state_bytes = peak;
+        rep->converged = 1;
+        rep->forward_ms = ms_fwd;
+        rep->adjoint_ms = ms_adj;
+        rep->sensitivity_ms = ms_sens;
+    }
+    return LBM_OK;
+}
+
+// Horizon adjoint with binomial checkpointing (scan.rs binomial_scan,
+// :285-390): the actions of revolve_plan drive the device state.  The forward
+// sweep is the admitted forward (every state's admission record, as
+// run_admitted); after its last step the state before it is still in the
+// other population array, which is where the reverse sweep starts.  A
+// reversed step k takes the record of state k-1 from a load-only pass and
+// applies the transposed step linearised there (with the state's stage seed
+// for the time-averaged objective).  One record slot suffices.
+lbm_status gradient_binomial(lbm_handle& h, const double* w, const lbm_adjoint_opts_t& o, double* grad,
+                             lbm_adjoint_report_t* rep) {
+    require_design(h);
+    const int64_t T = h.step_count;
+    const RevolvePlan plan = revolve_plan(T, o.snapshots);
+    const bool stage = o.objective == LBM_OBJ_TIME_AVERAGE;
+    const int rec_planes = stage ? 10 : 4;
+    alloc_adjoint(h, o.lambda_storage);
+    int64_t* ctr = &h.device_bytes;
+    h.record.fit((size_t)h.n() * rec_planes * sizeof(float) + CELL_PAD * sizeof(float), ctr);
+    const size_t ab = h.array_bytes(h.storage);
+    std::vector<Checkpoint> slots((size_t)o.snapshots);
+    auto store = [&](int64_t slot) {
+        Checkpoint& c = slots[(size_t)slot];
+        if (!c.buf) {
+            c.buf = std::make_unique<DevBuf>();
+            c.buf->alloc(ab, ctr);
+        }
+        CK(cudaMemcpyAsync(c.buf->p, h.pop_array(h.cur), ab, cudaMemcpyDeviceToDevice, h.stream));
+        c.t = h.t;
+        c.pending = h.pending;
+    };
+    auto need = [](bool ok) {
+        if (!ok) throw CudaError("binomial schedule and device state disagree");
+    };
+    // forward sweep with the admission record of every state
+    init_state(h);
+    h.diag.alloc((size_t)(T + 1) * sizeof(StepDiag), ctr);
+    StepDiag* d = h.diag.as<StepDiag>();
+    ensure_port_maps(h, T);
+    bool prev_pending = false;
+    CK(cudaEventRecord(h.ev0, h.stream));
+    for (size_t i = 0; i < plan.reverse_start; ++i) {
+        const RevolveAction& x = plan.actions[i];
+        if (x.kind == RevolveAction::SNAPSHOT) {
+            need(h.t == x.a);
+            store(x.b);
+        } else if (x.kind == RevolveAction::ADVANCE) {
+            need(h.t == x.a);
+            for (int64_t t = x.a; t < x.b; ++t) {
+                prev_pending = h.pending;
+                step(h, d + t, nullptr);
+            }
+        } else {
+            need(false);
+        }
+    }
+    need(h.t == T);
+    inspect(h, d + T, nullptr);
+    CK(cudaEventRecord(h.ev1, h.stream));
+    std::vector<StepDiag>& hd = h.last_trajectory;
+    hd.resize((size_t)T + 1);
+    CK(cudaMemcpyAsync(hd.data(), d, hd.size() * sizeof(StepDiag), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    float ms_sweep = 0;
+    CK(cudaEventElapsedTime(&ms_sweep, h.ev0, h.ev1));
+    check_errflag(h);
+    lbm_diag_t dg{};
+    admit(h, hd, &dg, ms_sweep);
+    h.forward_done = true;
+    AdjState st;
+    const double n0 = seed(h, w, st, nullptr, stage ? 1.0 / (double)T : 1.0);
+    const SeedParams sp = stage_seed(h, w, 1.0 / (double)T);
+    // back to state T-1, which the last step left in the other array
+    h.cur ^= 1;
+    h.t = T - 1;
+    h.pending = prev_pending;
+    int64_t rescale = 1;
+    while (rescale * rescale < T) ++rescale;
+    int64_t recomputed = 0, reversed = 0;
+    float ms_fwd = 0, ms_adj = 0;
+    if (n0 > 0 || stage) {
+        // event pairs around runs of forward-type work (steps, record passes,
+        // state copies) and adjoint steps, from a pool created up front (at
+        // most two runs per action)
+        std::vector<cudaEvent_t> evs(2 * (plan.actions.size() - plan.reverse_start) + 2);
+        for (auto& e : evs) CK(cudaEventCreate(&e));
+        size_t used = 0;
+        std::vector<int> kinds;  // 0 forward, 1 adjoint, per pair
+        int open = -1;
+        auto mark = [&](int kind) {
+            if (open == kind) return;
+            CK(cudaEventRecord(evs[used++], h.stream));
+            if (open >= 0) kinds.push_back(open);
+            open = kind;
+        };
+        for (size_t i = plan.reverse_start; i < plan.actions.size(); ++i) {
+            const RevolveAction& x = plan.actions[i];
+            switch (x.kind) {
+                case RevolveAction::RESTORE: {
+                    const Checkpoint& c = slots[(size_t)x.b];
+                    need(c.buf && c.t == x.a);
+                    mark(0);
+                    CK(cudaMemcpyAsync(h.pop_array(h.cur), c.buf->p, ab, cudaMemcpyDeviceToDevice, h.stream));
+                    h.t = c.t;
+                    h.pending = c.pending;
+                    break;
+                }
+                case RevolveAction::SNAPSHOT:
+                    need(h.t == x.a);
+                    mark(0);
+                    store(x.b);
+                    break;
+                case RevolveAction::ADVANCE:
+                    need(h.t == x.a);
+                    mark(0);
+                    for (int64_t t = x.a; t < x.b; ++t) step(h, nullptr, nullptr);
+                    recomputed += x.b - x.a;
+                    break;
+                case RevolveAction::REVERSE: {
+                    need(h.t == x.a - 1);
+                    const int64_t t = x.a - 1;
+                    mark(0);
+                    inspect(h, nullptr, h.record.as<float>(), stage);
+                    mark(1);
+                    ++reversed;
+                    const bool norm = reversed % rescale == 0;
+                    adjoint_step(h, st, h.record.as<float>(), norm, t, stage && t >= 1 ? &sp : nullptr, rec_planes);
+                    // keep the stored adjoint near unit RMS, as the segments of Every(K) do
+                    if (norm) st.target = next_scale(h, read_norm(h) / st.scale, st.scale);
+                    break;
+                }
+                case RevolveAction::RELEASE:
+                    break;
+            }
+        }
+        mark(-1);
+        CK(cudaStreamSynchronize(h.stream));
+        for (size_t k = 0; k < kinds.size(); ++k) {
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, evs[k], evs[k + 1]));
+            (kinds[k] == 0 ? ms_fwd : ms_adj) += ms;
+        }
+        for (cudaEvent_t e : evs) cudaEventDestroy(e);
+    }
+    int64_t held = 0;
+    for (auto& c : slots)
+        if (c.buf) held += (int64_t)c.buf->bytes;
+    const int64_t peak = (int64_t)h.record.bytes + held;
+    slots.clear();
     h.forward_done = false;
     h.state_valid = false;
     check_errflag(h);
@@ -1650,6 +1830,19 @@ lbm_status lbm_responses(lbm_handle* h, double* out8) {
     });
 }
 
+lbm_status lbm_binomial_plan(int64_t steps, int64_t snapshots, int64_t* forward_steps, int64_t* peak_snapshots) {
+    try {
+        const RevolvePlan p = revolve_plan(steps, snapshots);
+        if (forward_steps) *forward_steps = p.forward_steps;
+        if (peak_snapshots) *peak_snapshots = p.peak;
+        return LBM_OK;
+    } catch (const std::invalid_argument&) {
+        return LBM_E_CONTRACT;
+    } catch (...) {
+        return LBM_E_STATE;
+    }
+}
+
 lbm_status lbm_time_average(lbm_handle* h, double* out8) {
     return guarded(h, [&]() {
         if (!h->time_average) throw ContractError("time averages need a problem created with time_average");
@@ -1713,6 +1906,11 @@ lbm_status lbm_gradient(lbm_handle* h, const double* weights, const lbm_adjoint_
             return gradient_steady(*h, weights, o, grad, report);
         }
         if (o.mode != LBM_ADJ_HORIZON) throw ContractError("adjoint mode must be horizon or steady");
+        if (o.checkpointing == LBM_CKPT_BINOMIAL) {
+            if (o.snapshots < 1) throw ContractError("binomial checkpointing needs at least one snapshot");
+            return gradient_binomial(*h, weights, o, grad, report);
+        }
+        if (o.checkpointing != LBM_CKPT_EVERY) throw ContractError("checkpointing must be every or binomial");
         return gradient_horizon(*h, weights, o, grad, report);
     });
 }

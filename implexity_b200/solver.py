@@ -94,6 +94,16 @@ class AdjointReport:
     sensitivity_ms: float
 
 
+def binomial_plan(steps: int, snapshots: int) -> tuple[int, int]:
+    """(forward steps, peak snapshots) of the binomial checkpoint schedule
+    (host only; implexity-ad/src/revolve.rs BinomialSchedule)."""
+    fw, pk = C.c_int64(), C.c_int64()
+    st = _abi.load().lbm_binomial_plan(int(steps), int(snapshots), C.byref(fw), C.byref(pk))
+    if st != 0:
+        raise ContractError(f"no binomial schedule for {steps} steps and {snapshots} snapshots")
+    return int(fw.value), int(pk.value)
+
+
 class LbmSolver:
     def __init__(self, problem: dict | NormalizedProblem):
         self.problem = problem if isinstance(problem, NormalizedProblem) else normalize(problem)
@@ -219,10 +229,14 @@ class LbmSolver:
         check_every: int = 50,
         objective: str = "final",
         record_budget_bytes: int = 0,
+        checkpointing: str = "every",
+        snapshots: int = 0,
     ) -> tuple[np.ndarray, AdjointReport]:
         """Design gradient of w . responses: of the final state (objective
         "final") or of their mean over the horizon's states ("time_average",
-        horizon mode, problems with solver_options.time_average)."""
+        horizon mode, problems with solver_options.time_average).  Horizon
+        checkpointing is a state every `checkpoint_every` steps ("every") or
+        the binomial schedule over `snapshots` states ("binomial")."""
         w = np.zeros(_abi.N_RESPONSES)
         w[: len(weights)] = np.asarray(weights, dtype=float)
         o = _abi.AdjointOpts()
@@ -234,6 +248,8 @@ class LbmSolver:
         o.tolerance = float(tolerance)
         o.record_budget_bytes = int(record_budget_bytes)
         o.objective = {"final": _abi.LBM_OBJ_FINAL, "time_average": _abi.LBM_OBJ_TIME_AVERAGE}[objective]
+        o.checkpointing = {"every": _abi.LBM_CKPT_EVERY, "binomial": _abi.LBM_CKPT_BINOMIAL}[checkpointing]
+        o.snapshots = int(snapshots)
         grad = np.empty(self.shape)
         rep = _abi.AdjointReport()
         st = self.lib.lbm_gradient(self.h, _dp(w), C.byref(o), _dp(grad), C.byref(rep))

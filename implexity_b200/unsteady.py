@@ -9,11 +9,12 @@ horizon adjoint with a checkpoint every K steps (scan.rs Every(K)); when a
 segment's per-step records do not fit in device memory, each segment is split
 once more (a second checkpoint level).  For every K the report gives the
 device bytes of checkpoints + records, the recomputed forward steps and the
-device times.
+device times; the binomial schedule (revolve) with a given number of stored
+states is reported the same way.
 
 Command line (one GPU)::
 
-    python -m implexity_b200.unsteady --shape 192 192 192 --steps 4000 --K 50 200 800
+    python -m implexity_b200.unsteady --shape 192 192 192 --steps 4000 --K 50 200 800 --snapshots 10 40
 """
 from __future__ import annotations
 
@@ -37,7 +38,8 @@ def weights(objective: str) -> np.ndarray:
     return workloads.objective_weights()
 
 
-def run(shape, steps, Ks, period_steps=1000, storage="float32", seed=0, objective="dissipation", log=print):
+def run(shape, steps, Ks, period_steps=1000, storage="float32", seed=0, objective="dissipation", log=print,
+        snapshots=()):
     prob = workloads.pulsatile_problem(shape=tuple(shape), steps=steps, lattice="D3Q27", period_steps=period_steps,
                                        storage=storage)
     norm = normalize(prob)
@@ -70,6 +72,18 @@ def run(shape, steps, Ks, period_steps=1000, storage="float32", seed=0, objectiv
                    "grad_rel_l2_vs_first_K": float(np.linalg.norm(g - g_first) / np.linalg.norm(g_first))}
             log(json.dumps(rec))
             out.append(rec)
+        for S in snapshots:
+            t0 = time.perf_counter()
+            g, rep = s.gradient(w, mode="horizon", checkpointing="binomial", snapshots=S, objective="time_average",
+                                lambda_storage=storage)
+            wall = time.perf_counter() - t0
+            rec = {"binomial_snapshots": S, "peak_state_GB": rep.peak_state_bytes / 1e9,
+                   "forward_recomputed": rep.forward_recomputed, "adjoint_steps": rep.iterations,
+                   "recompute_ms": rep.forward_ms, "adjoint_ms": rep.adjoint_ms, "wall_s": wall,
+                   "grad_rel_l2_vs_first_K": (float(np.linalg.norm(g - g_first) / np.linalg.norm(g_first))
+                                              if g_first is not None else None)}
+            log(json.dumps(rec))
+            out.append(rec)
     return base, out
 
 
@@ -81,8 +95,10 @@ def main():
     ap.add_argument("--period-steps", type=int, default=1000)
     ap.add_argument("--storage", choices=["float32", "float16"], default="float32")
     ap.add_argument("--objective", choices=["dissipation", "channel"], default="dissipation")
+    ap.add_argument("--snapshots", type=int, nargs="*", default=[],
+                    help="also run the binomial schedule with these numbers of stored states")
     a = ap.parse_args()
-    run(a.shape, a.steps, a.K, a.period_steps, a.storage, objective=a.objective)
+    run(a.shape, a.steps, a.K, a.period_steps, a.storage, objective=a.objective, snapshots=a.snapshots)
 
 
 if __name__ == "__main__":

@@ -49,7 +49,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 2
+#define LBM_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define LBM_API __attribute__((visibility("default")))
@@ -210,6 +210,13 @@ typedef enum { LBM_ADJ_HORIZON = 0, LBM_ADJ_STEADY = 1 } lbm_adjoint_mode;
  * adjoint; HORIZON mode, problems created with time_average). */
 typedef enum { LBM_OBJ_FINAL = 0, LBM_OBJ_TIME_AVERAGE = 1 } lbm_objective;
 
+/* Checkpointing of the HORIZON adjoint (implexity-ad/src/scan.rs:108-116,
+ * Checkpointing).  EVERY stores the state every checkpoint_every steps
+ * (Every(K)); BINOMIAL keeps at most `snapshots` states and follows the
+ * binomial (revolve) schedule of implexity-ad/src/revolve.rs:128-330, which
+ * minimises the recomputed steps for that number of states. */
+typedef enum { LBM_CKPT_EVERY = 0, LBM_CKPT_BINOMIAL = 1 } lbm_checkpointing;
+
 typedef struct {
     int32_t mode;             /* lbm_adjoint_mode */
     int32_t lambda_storage;   /* lbm_storage of the adjoint populations */
@@ -219,6 +226,8 @@ typedef struct {
     double tolerance;         /* STEADY: relative residual */
     int64_t record_budget_bytes; /* HORIZON: device bytes for per-step records (0 = auto) */
     int32_t objective;        /* lbm_objective */
+    int32_t checkpointing;    /* HORIZON: lbm_checkpointing */
+    int64_t snapshots;        /* HORIZON, BINOMIAL: state slots (>= 1) */
 } lbm_adjoint_opts_t;
 
 typedef struct {
@@ -311,6 +320,14 @@ LBM_API lbm_status lbm_time_average(lbm_handle* h, double* out8);
 LBM_API lbm_status lbm_fields(lbm_handle* h, double* density, double* velocity, double* pressure);
 
 /* ---- adjoint ------------------------------------------------------------ */
+
+/* The binomial checkpoint schedule for `steps` steps and `snapshots` state
+ * slots (BinomialSchedule::new, implexity-ad/src/revolve.rs:247-283), built
+ * on the host: the forward steps it takes in all (optimal_forward_steps,
+ * revolve.rs:117-125) and the most slots it holds at once.  Host only; no
+ * device is needed. */
+LBM_API lbm_status lbm_binomial_plan(int64_t steps, int64_t snapshots, int64_t* forward_steps,
+                                     int64_t* peak_snapshots);
 
 /* Design gradient of sum_k weights[k] * response_k (weights has
  * LBM_N_RESPONSES entries) with respect to the raw design, after a
