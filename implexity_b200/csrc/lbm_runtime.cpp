@@ -373,7 +373,14 @@ struct lbm_handle {
     }
     char* pop_array(int k) const { return static_cast<char*>(pop.p) + (size_t)k * array_bytes(storage); }
     // planes start after the front padding: current (A) and other (B) array
-    void* popA() const { return pop_array(cur) + pop_pad(G) * (storage == LBM_STORE_F32 ? 4 : 2); }
+    // A stored state (a checkpoint buffer laid out like a population array)
+    // that stands for the current state until the next step: the step reads
+    // it in place of the current array, so restoring a state needs no copy.
+    const char* restored = nullptr;
+    void* popA() const {
+        const char* base = restored ? restored : pop_array(cur);
+        return const_cast<char*>(base) + pop_pad(G) * (storage == LBM_STORE_F32 ? 4 : 2);
+    }
     void* popB() const { return pop_array(cur ^ 1) + pop_pad(G) * (storage == LBM_STORE_F32 ? 4 : 2); }
     void* lam_plane0(int k) const {
         return static_cast<char*>(lam.p) + (size_t)k * array_bytes(lam_storage) +
@@ -809,6 +816,7 @@ void step(lbm_handle& h, StepDiag* diag, float* record, bool record_s = false, d
     a.step = (uint32_t)h.t;
     CK(launch_forward(h.Q, coll_kind(h), h.storage, a, grid_for(h), h.stream));
     h.cur ^= 1;
+    h.restored = nullptr;
     h.pending = h.n_ports > 0;
     ++h.t;
 }
@@ -1459,13 +1467,20 @@ lbm_status gradient_binomial(lbm_handle& h, const double* w, const lbm_adjoint_o
     h.record.fit((size_t)h.n() * rec_planes * sizeof(float) + CELL_PAD * sizeof(float), ctr);
     const size_t ab = h.array_bytes(h.storage);
     std::vector<Checkpoint> slots((size_t)o.snapshots);
+    // a restored slot stands for the current state only while the slots live
+    // (declared after them, so it is cleared first on every exit path)
+    struct ClearRestored {
+        lbm_handle& h;
+        ~ClearRestored() { h.restored = nullptr; }
+    } clear_restored{h};
     auto store = [&](int64_t slot) {
         Checkpoint& c = slots[(size_t)slot];
         if (!c.buf) {
             c.buf = std::make_unique<DevBuf>();
             c.buf->alloc(ab, ctr);
         }
-        CK(cudaMemcpyAsync(c.buf->p, h.pop_array(h.cur), ab, cudaMemcpyDeviceToDevice, h.stream));
+        const char* cur = h.restored ? h.restored : h.pop_array(h.cur);
+        CK(cudaMemcpyAsync(c.buf->p, cur, ab, cudaMemcpyDeviceToDevice, h.stream));
         c.t = h.t;
         c.pending = h.pending;
     };
@@ -1537,10 +1552,10 @@ lbm_status gradient_binomial(lbm_handle& h, const double* w, const lbm_adjoint_o
             const RevolveAction& x = plan.actions[i];
             switch (x.kind) {
                 case RevolveAction::RESTORE: {
+                    // the next step or record pass reads the slot in place
                     const Checkpoint& c = slots[(size_t)x.b];
                     need(c.buf && c.t == x.a);
-                    mark(0);
-                    CK(cudaMemcpyAsync(h.pop_array(h.cur), c.buf->p, ab, cudaMemcpyDeviceToDevice, h.stream));
+                    h.restored = static_cast<const char*>(c.buf->p);
                     h.t = c.t;
                     h.pending = c.pending;
                     break;
@@ -1582,6 +1597,7 @@ lbm_status gradient_binomial(lbm_handle& h, const double* w, const lbm_adjoint_o
         }
         for (cudaEvent_t e : evs) cudaEventDestroy(e);
     }
+    h.restored = nullptr;
     int64_t held = 0;
     for (auto& c : slots)
         if (c.buf) held += (int64_t)c.buf->bytes;
