@@ -147,15 +147,15 @@ def run_gpu(args, rank, world, local):
     torch.cuda.set_device(local)
     from implexity_b200 import LbmSolver, normalize, workloads
 
-    shape, T, coll, bulk, dkind = CONFIGS[args.config]
+    shape, T, coll = CONFIGS[args.config][:3]
     variants = [v for v in args.variants.split(",") if v]
     results = {}
     hbm, peak_kind = peaks()
     for variant in variants:
         storage = "float16" if variant == "fp16" else "float32"
-        prob = workloads.channel_problem(shape=shape, steps=T, collision=coll, storage=storage, mrt_bulk_rate=bulk)
+        prob = workloads.config_problem(args.config, storage=storage)
         norm = normalize(prob)
-        raw = (workloads.uniform_design(shape, 0) if dkind == "uniform" else workloads.sphere_design(shape, 0))
+        raw = workloads.config_design(args.config, 0)
         raw_pinned = torch.from_numpy(raw).pin_memory().numpy()
         w = workloads.objective_weights()
         s = LbmSolver(norm)
@@ -241,12 +241,10 @@ def run_profile_case(args):
     from implexity_b200 import ConvergenceError, LbmSolver, normalize, workloads
 
     torch.cuda.set_device(0)
-    shape, T, coll, bulk, dkind = CONFIGS[args.config]
     storage = "float16" if args.variants.split(",")[0] == "fp16" else "float32"
-    prob = workloads.channel_problem(shape=shape, steps=args.forward_steps, collision=coll, storage=storage,
-                                     mrt_bulk_rate=bulk)
+    prob = workloads.config_problem(args.config, storage=storage, steps=args.forward_steps)
     s = LbmSolver(normalize(prob))
-    raw = workloads.uniform_design(shape, 0) if dkind == "uniform" else workloads.sphere_design(shape, 0)
+    raw = workloads.config_design(args.config, 0)
     s.set_design(raw)
     d = s.forward()
     try:
@@ -265,11 +263,10 @@ def cpu_sample(config, seconds_target=15.0, threads=None):
 
     if threads:
         orc.set_threads(threads)
-    shape, T, coll, bulk, dkind = CONFIGS[config]
-    prob = workloads.channel_problem(shape=shape, steps=T, collision=coll, mrt_bulk_rate=bulk)
+    prob = workloads.config_problem(config)
     norm = normalize(prob)
     o = orc.Oracle(norm)
-    raw = workloads.uniform_design(shape, 0) if dkind == "uniform" else workloads.sphere_design(shape, 0)
+    raw = workloads.config_design(config, 0)
     phi, alpha = o.design(raw)
     f = o.initial()
     lam = np.random.default_rng(0).standard_normal(f.shape) * 1e-3

@@ -123,10 +123,10 @@ def taylor_test(solver: LbmSolver, raw: np.ndarray, weights: np.ndarray, gradien
 def run(config: str, count: int, step: float, seed: int, mode: str, checkpoint_every: int,
         tolerance: float, storage: str = "float32") -> dict:
     """The gradient check of a bench workload; returns a JSON-ready report."""
-    shape, steps, coll, bulk, dkind = workloads.CONFIGS[config]
-    prob = workloads.channel_problem(shape=shape, steps=steps, collision=coll, storage=storage, mrt_bulk_rate=bulk)
+    shape = workloads.CONFIGS[config][0]
+    prob = workloads.config_problem(config, storage=storage)
     norm = normalize(prob)
-    raw = workloads.uniform_design(shape, 0) if dkind == "uniform" else workloads.sphere_design(shape, 0)
+    raw = workloads.config_design(config, 0)
     w = workloads.objective_weights()
     editable = (np.asarray(norm.design_region, bool) & ~np.asarray(norm.solid_mask, bool)).reshape(shape)
     t0 = time.perf_counter()

@@ -26,8 +26,30 @@ CONFIGS = {
     "channel48x24x24_trt": ((48, 24, 24), 2000, "trt", None, "uniform"),
     "channel64_trt": ((64, 64, 64), 5000, "trt", None, "uniform"),
 }
+# Relaxation time where it is not the channel's 0.8: the MRT sphere workload
+# relaxes shear at rate 1.0 (tau = 1) and bulk at 1.2.
+CONFIG_TAU = {"channel256x128x128_mrt": 1.0}
 # The unsteady D3Q27 workload: shape, steps, inlet period in steps.
 PULSATILE = {"pulsatile192_d3q27": ((192, 192, 192), 4000, 1000)}
+
+
+def config_problem(name: str, storage: str = "float32", steps: int | None = None, shape=None, **kw) -> dict:
+    """The problem of a named workload (optionally with another step count,
+    grid shape or channel_problem keyword, for reduced-size checks)."""
+    shp, T, coll, bulk, _ = CONFIGS[name]
+    return channel_problem(shape=tuple(shape) if shape is not None else shp, steps=T if steps is None else steps,
+                           collision=coll, storage=storage, mrt_bulk_rate=bulk, tau=CONFIG_TAU.get(name, 0.8), **kw)
+
+
+def config_design(name: str, seed: int = 0, shape=None) -> np.ndarray:
+    """The seeded raw design of a named workload.  On another grid shape the
+    sphere radii scale with the grid, so the blocked volume stays the same."""
+    full, _, _, _, kind = CONFIGS[name]
+    shp = tuple(shape) if shape is not None else full
+    if kind == "uniform":
+        return uniform_design(shp, seed)
+    f = shp[0] / full[0]
+    return sphere_design(shp, seed, rmin=4.0 * f, rmax=12.0 * f)
 
 
 def channel_problem(
