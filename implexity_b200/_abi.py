@@ -42,6 +42,7 @@ EXPORTS = [
     "lbm_responses",
     "lbm_time_average",
     "lbm_binomial_plan",
+    "lbm_probe_bounded_wait",
     "lbm_fields",
     "lbm_gradient",
     "lbm_step_vjp",
@@ -176,6 +177,7 @@ def _declare(lib: C.CDLL) -> None:
     lib.lbm_responses.argtypes = [h, _dp]
     lib.lbm_time_average.argtypes = [h, _dp]
     lib.lbm_binomial_plan.argtypes = [C.c_int64, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.lbm_probe_bounded_wait.argtypes = [C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
     lib.lbm_fields.argtypes = [h, _dp, _dp, _dp]
     lib.lbm_gradient.argtypes = [h, _dp, C.POINTER(AdjointOpts), _dp, C.POINTER(AdjointReport)]
     lib.lbm_step_vjp.argtypes = [h, _dp, _dp, _dp, _dp, C.c_size_t]

@@ -141,6 +141,7 @@ cudaError_t launch_init(int Q, int storage, const Geometry& G, const Physics& P,
                         cudaStream_t s);
 cudaError_t launch_forward(int Q, int coll, int storage, const FwdArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_adjoint(int Q, int coll, int lstorage, const AdjArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_wait_probe(int* err, uint64_t limit_ns, unsigned long long* waited_ns, cudaStream_t s);
 cudaError_t launch_objective(int Q, int storage, int lstorage, int mode, const ObjArgs& a, int grid,
                              cudaStream_t s);  // mode 0: responses/fields, 1: seed
 cudaError_t launch_canon_pop(int Q, int storage, const Geometry& G, const void* pop, const uint32_t* mask,

@@ -236,6 +236,24 @@ __global__ void __launch_bounds__(BLOCK) k_seed_lam(Geometry G, T* B, const uint
     }
 }
 
+// ------------------------------------------------------------------ bounded-wait probe
+// One thread waits on an mbarrier that nothing arrives at, with the stepping
+// kernels' bounded wait and a short limit: the wait must give up, set the
+// error flag and return, leaving the context usable.
+__global__ void k_wait_probe(int* err, uint64_t limit_ns, unsigned long long* waited_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint64_t t0 = global_ns();
+        mbar_wait(&bar, 0, err, limit_ns);
+        *waited_ns = global_ns() - t0;
+    }
+}
+
 // ------------------------------------------------------------------ design
 __device__ __forceinline__ bool shifted(const Geometry& G, int64_t x, int dx, int dy, int dz, int64_t& out) {
     int64_t i, j, k;
@@ -357,6 +375,11 @@ static void objective_dispatch(int lstorage, int mode, const ObjArgs& a, int gri
     } else {
         LBM_STORAGE_DISPATCH(lstorage, TL, k_objective<Q, T, TL, 1><<<persistent_grid((const void*)k_objective<Q, T, TL, 1>, a.G.n), BLOCK, 0, s>>>(a))
     }
+}
+
+cudaError_t launch_wait_probe(int* err, uint64_t limit_ns, unsigned long long* waited_ns, cudaStream_t s) {
+    k_wait_probe<<<1, 32, 0, s>>>(err, limit_ns, waited_ns);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_objective(int Q, int storage, int lstorage, int mode, const ObjArgs& a, int grid,

@@ -1846,6 +1846,31 @@ lbm_status lbm_responses(lbm_handle* h, double* out8) {
     });
 }
 
+lbm_status lbm_probe_bounded_wait(int64_t limit_ns, int32_t* timed_out, double* waited_ms) {
+    if (!timed_out || limit_ns < 1000000 || limit_ns > 1000000000) return LBM_E_CONTRACT;
+    int* err = nullptr;
+    unsigned long long* waited = nullptr;
+    lbm_status st = LBM_OK;
+    auto ok = [&](cudaError_t e) {
+        if (e != cudaSuccess && st == LBM_OK) st = LBM_E_CUDA;
+        return e == cudaSuccess;
+    };
+    if (ok(cudaMalloc(&err, sizeof(int))) && ok(cudaMalloc(&waited, sizeof(unsigned long long))) &&
+        ok(cudaMemset(err, 0, sizeof(int))) && ok(launch_wait_probe(err, (uint64_t)limit_ns, waited, 0)) &&
+        ok(cudaDeviceSynchronize())) {
+        int e = 0;
+        unsigned long long ns = 0;
+        if (ok(cudaMemcpy(&e, err, sizeof(int), cudaMemcpyDeviceToHost)) &&
+            ok(cudaMemcpy(&ns, waited, sizeof(ns), cudaMemcpyDeviceToHost))) {
+            *timed_out = e ? 1 : 0;
+            if (waited_ms) *waited_ms = (double)ns * 1e-6;
+        }
+    }
+    if (err) cudaFree(err);
+    if (waited) cudaFree(waited);
+    return st;
+}
+
 lbm_status lbm_binomial_plan(int64_t steps, int64_t snapshots, int64_t* forward_steps, int64_t* peak_snapshots) {
     try {
         const RevolvePlan p = revolve_plan(steps, snapshots);

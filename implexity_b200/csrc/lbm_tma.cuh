@@ -59,21 +59,21 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// Polls until the phase completes or kWaitNs have passed since t0.
-__device__ __forceinline__ bool mbar_poll_until(uint64_t* bar, uint32_t parity, uint64_t t0) {
+// Polls until the phase completes or limit_ns have passed since t0.
+__device__ __forceinline__ bool mbar_poll_until(uint64_t* bar, uint32_t parity, uint64_t t0, uint64_t limit_ns) {
     while (true) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (global_ns() - t0 > kWaitNs) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     }
 }
 
 // Bounded wait for the phase with the given parity.  Returns false (and sets
 // *err) if the copies did not land within the limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, uint64_t limit_ns = kWaitNs) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (mbar_poll_until(bar, parity, global_ns())) return true;
+    if (mbar_poll_until(bar, parity, global_ns(), limit_ns)) return true;
     if (err) atomicOr(err, 1);
-    mbar_poll_until(bar, parity, global_ns());
+    mbar_poll_until(bar, parity, global_ns(), limit_ns);
     return false;
 }
 

@@ -27,7 +27,7 @@ import numpy as np
 
 from . import workloads
 from .mma import MmaOptimizer
-from .problem import normalize
+from .problem import ContractError, normalize
 from .solver import LbmSolver
 
 
@@ -90,9 +90,18 @@ class DesignLoop:
         x = raw[self.free].copy()
         xm1 = xm2 = x.copy()
         history = []
+        stopped = None
         for it in range(iterations):
             t0 = time.perf_counter()
-            f0, g, con, dcon, timing = self.evaluate(raw)
+            try:
+                f0, g, con, dcon, timing = self.evaluate(raw)
+            except ContractError as e:
+                # the reference driver fails the job when an evaluation is
+                # refused (admission); the loop stops here and keeps its history
+                stopped = {"iteration": it, "stopped": str(e)}
+                if log:
+                    log(stopped)
+                break
             df0 = g[self.free]
             fs = np.array([con])
             dfs = dcon[self.free][None, :]
@@ -110,7 +119,7 @@ class DesignLoop:
                 log(rec)
             xm2, xm1, x = xm1, x, xn
             raw[self.free] = x
-        return {"history": history, "final_design": raw}
+        return {"history": history, "final_design": raw, "stopped": stopped}
 
 
 def c5_problem(shape=(512, 256, 256), forward_steps=3000, storage="float32"):
@@ -142,6 +151,7 @@ def main():
         loop.close()
     h = out["history"]
     print(json.dumps({"design_loop": list(shape), "storage": a.storage, "iterations": len(h),
+                      "stopped": out["stopped"],
                       "objective": [r["objective"] for r in h], "volume_fraction": [r["volume_fraction"] for r in h],
                       "wall_s_per_iteration": [r["wall_s"] for r in h], "mma_s": [r["mma_s"] for r in h]}))
 

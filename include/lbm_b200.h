@@ -319,6 +319,14 @@ LBM_API lbm_status lbm_time_average(lbm_handle* h, double* out8);
  * Any pointer may be NULL. */
 LBM_API lbm_status lbm_fields(lbm_handle* h, double* density, double* velocity, double* pressure);
 
+/* Diagnostic, no counterpart in the reference: runs one bounded wait of the
+ * stepping kernels (an mbarrier wait with the given limit) on an mbarrier that
+ * nothing completes, on the current device.  The wait must run out: then
+ * *timed_out = 1 and *waited_ms is the device time the wait took (one period
+ * of limit_ns waiting before the error flag is set, one more before the
+ * kernel returns).  limit_ns in [1e6, 1e9]. */
+LBM_API lbm_status lbm_probe_bounded_wait(int64_t limit_ns, int32_t* timed_out, double* waited_ms);
+
 /* ---- adjoint ------------------------------------------------------------ */
 
 /* The binomial checkpoint schedule for `steps` steps and `snapshots` state

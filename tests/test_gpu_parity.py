@@ -292,3 +292,19 @@ def test_periodic_solid_horizon_gradient_matches_oracle(gpu_lib):
         s.set_design(raw)
         g, _ = s.gradient(w, mode="horizon", checkpoint_every=9)
     assert rel_l2(g, g_ref) < 1e-4, rel_l2(g, g_ref)
+
+
+def test_bounded_wait_runs_out_and_the_context_stays_usable(gpu_lib):
+    """A wait that nothing completes gives up after its limit, reports it
+    through the error flag and returns; the next solve runs normally."""
+    import ctypes as C
+
+    timed_out, waited = C.c_int32(0), C.c_double(0.0)
+    assert gpu_lib.lbm_probe_bounded_wait(50_000_000, C.byref(timed_out), C.byref(waited)) == 0
+    assert timed_out.value == 1
+    assert 50.0 <= waited.value < 2000.0, waited.value
+    prob, norm, raw = make("trt", "D3Q19", steps=20)
+    with LbmSolver(prob) as s:
+        s.set_design(raw)
+        d = s.forward()
+        assert d.admitted
