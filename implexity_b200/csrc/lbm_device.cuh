@@ -24,6 +24,7 @@
 // same pattern: the AA scheme run with the velocities reversed (pull from
 // x + c_q), linearised at a recorded (rho, u).
 #pragma once
+#include <type_traits>
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -122,6 +123,34 @@ template <typename T>
 __device__ __forceinline__ T senc_sr(float v, uint32_t& rs) {
     if constexpr (Cvt<T>::scaled) return round_stochastic<T>(v, lcg(rs));
     else return Cvt<T>::from(v);
+}
+
+// Two values to FP16 with stochastic rounding in one conversion (sm_100a
+// cvt.rs): `hi` lands in the upper half, `lo` in the lower, each rounded
+// with random bits taken from rbits.
+__device__ __forceinline__ uint32_t sr_half2(float hi, float lo, uint32_t rbits) {
+    uint32_t d;
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+    return d;
+}
+
+// All Q values of a cell in storage units -> stored elements, handed to
+// put(q, element).  FP16 converts the directions in pairs (one random word
+// per pair); the other formats one by one.
+template <int Q, typename T, typename Put>
+__device__ __forceinline__ void senc_sr_all(const float (&v)[Q], uint32_t& rs, Put&& put) {
+    if constexpr (std::is_same<T, __half>::value) {
+#pragma unroll
+        for (int q = 0; q + 1 < Q; q += 2) {
+            const uint32_t d = sr_half2(v[q + 1], v[q], lcg(rs));
+            put(q, __ushort_as_half((unsigned short)(d & 0xffffu)));
+            put(q + 1, __ushort_as_half((unsigned short)(d >> 16)));
+        }
+        if constexpr (Q % 2) put(Q - 1, round_stochastic<T>(v[Q - 1], lcg(rs)));
+    } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) put(q, senc_sr<T>(v[q], rs));
+    }
 }
 
 // ------------------------------------------------------------------ indexing
@@ -1057,8 +1086,7 @@ template <int Q, typename T>
 __device__ __forceinline__ void store_own_pop(T* A, uint32_t n, uint32_t x, const float (&v)[Q], uint32_t step) {
     uint32_t rs = 0;
     if constexpr (Cvt<T>::scaled) rs = cell_seed(x, step);
-#pragma unroll
-    for (int q = 0; q < Q; ++q) A[q * n + x] = senc_sr<T>(v[q], rs);
+    senc_sr_all<Q, T>(v, rs, [&](int q, T e) { A[q * n + x] = e; });
 }
 
 template <int Q, typename T>

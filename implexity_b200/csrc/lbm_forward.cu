@@ -193,8 +193,7 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
                 } else if (fluid) {
                     uint32_t rs = 0;
                     if constexpr (Cvt<T>::scaled) rs = cell_seed(x, a.step);
-#pragma unroll
-                    for (int q = 0; q < Q; ++q) st->run[q][c] = senc_sr<T>(v[q], rs);
+                    senc_sr_all<Q, T>(v, rs, [&](int q, T e) { st->run[q][c] = e; });
                 } else {
 #pragma unroll
                     for (int q = 0; q < Q; ++q) st->run[q][c] = A[q * n + x];
