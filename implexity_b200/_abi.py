@@ -43,6 +43,7 @@ EXPORTS = [
     "lbm_time_average",
     "lbm_binomial_plan",
     "lbm_probe_bounded_wait",
+    "lbm_wall_loads",
     "lbm_fields",
     "lbm_gradient",
     "lbm_step_vjp",
@@ -178,6 +179,7 @@ def _declare(lib: C.CDLL) -> None:
     lib.lbm_time_average.argtypes = [h, _dp]
     lib.lbm_binomial_plan.argtypes = [C.c_int64, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.lbm_probe_bounded_wait.argtypes = [C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+    lib.lbm_wall_loads.argtypes = [h, C.c_double, _dp, _dp, _dp, C.c_size_t, C.POINTER(C.c_size_t)]
     lib.lbm_fields.argtypes = [h, _dp, _dp, _dp]
     lib.lbm_gradient.argtypes = [h, _dp, C.POINTER(AdjointOpts), _dp, C.POINTER(AdjointReport)]
     lib.lbm_step_vjp.argtypes = [h, _dp, _dp, _dp, _dp, C.c_size_t]

@@ -148,6 +148,10 @@ cudaError_t launch_canon_pop(int Q, int storage, const Geometry& G, const void* 
                              const PortMap* ports, int apply_ports, float* out, int grid, cudaStream_t s);
 cudaError_t launch_upload_pop(int Q, int storage, const Geometry& G, void* pop, const uint32_t* mask,
                               const float* in, int grid, cudaStream_t s);
+cudaError_t launch_wall_loads(int Q, int storage, const Geometry& G, const Physics& P, const void* A,
+                              const uint32_t* mask, const float* alpha, const PortMap* ports, int apply_ports,
+                              const uint32_t* cells, const uint8_t* links, int64_t n_links, double* out,
+                              cudaStream_t s);
 cudaError_t launch_canon_lam(int Q, int lstorage, const Geometry& G, const void* lam, const uint32_t* mask,
                              float inv_scale, float* out, int grid, cudaStream_t s);
 cudaError_t launch_seed_lam(int Q, int lstorage, const Geometry& G, void* lam, const uint32_t* mask,

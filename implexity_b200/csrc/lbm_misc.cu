@@ -3,6 +3,8 @@
 // conversions, the design map and its transpose.  Streamed states are read
 // through the pull of the stepping kernels and written through its inverse
 // scatter (pull_index, lbm_device.cuh).
+#include <algorithm>
+
 #include "lbm_device.cuh"
 
 namespace lbm {
@@ -236,6 +238,34 @@ __global__ void __launch_bounds__(BLOCK) k_seed_lam(Geometry G, T* B, const uint
     }
 }
 
+// ------------------------------------------------------------------ wall loads
+// Fixed-wall momentum exchange of the last interval (wall_exchange.rs:79-100):
+// the state before the last step is pulled again from the previous array
+// (with its port reconstruction), collided with the Guo-BGK collision that
+// the reference's loads use whatever the problem's collision
+// (solver::collide), and each listed blocked link (cell, q) gets the
+// outgoing population g*_opp(q) = f*_opp(q) - w_opp(q).
+template <int Q, typename T>
+__global__ void __launch_bounds__(BLOCK) k_wall_loads(Geometry G, Physics P, const T* A, const uint32_t* __restrict__ mask,
+                                                      const float* __restrict__ alpha, const PortMap* ports,
+                                                      int apply_ports, const uint32_t* cells, const uint8_t* links,
+                                                      int64_t n_links, double* out) {
+    for (int64_t i = (int64_t)blockIdx.x * BLOCK + threadIdx.x; i < n_links; i += (int64_t)gridDim.x * BLOCK) {
+        const uint32_t x = cells[i];
+        const int q = links[i];
+        const uint32_t m = mask[x];
+        float g[Q];
+        load_pop<Q, T>(A, G, x, m, g);
+        if (apply_ports && (m & MASK_PORT)) apply_port<Q>(ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], g);
+        collide_fused<Q, CK_PAIRS, 0>(g, alpha[x], P, true);
+        float o = 0.f;
+#pragma unroll
+        for (int r = 0; r < Q; ++r)
+            if (r == opp<Q>(q)) o = g[r];
+        out[i] = (double)o;
+    }
+}
+
 // ------------------------------------------------------------------ bounded-wait probe
 // One thread waits on an mbarrier that nothing arrives at, with the stepping
 // kernels' bounded wait and a short limit: the wait must give up, set the
@@ -414,6 +444,28 @@ cudaError_t launch_upload_pop(int Q, int storage, const Geometry& G, void* pop, 
     } else {
         LBM_STORAGE_DISPATCH(storage, T,
                              k_upload_pop<27, T><<<grid, BLOCK, 0, s>>>(G, static_cast<T*>(pop), mask, in))
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wall_loads(int Q, int storage, const Geometry& G, const Physics& P, const void* A,
+                              const uint32_t* mask, const float* alpha, const PortMap* ports, int apply_ports,
+                              const uint32_t* cells, const uint8_t* links, int64_t n_links, double* out,
+                              cudaStream_t s) {
+    if (n_links <= 0) return cudaSuccess;
+    const int grid = (int)std::min<int64_t>((n_links + BLOCK - 1) / BLOCK, 4096);
+    Physics B = P;
+    B.om = B.omega;  // BGK: both pair rates equal the shear rate
+    if (Q == 19) {
+        LBM_STORAGE_DISPATCH(storage, T,
+                             k_wall_loads<19, T><<<grid, BLOCK, 0, s>>>(G, B, static_cast<const T*>(A), mask, alpha,
+                                                                         ports, apply_ports, cells, links, n_links,
+                                                                         out))
+    } else {
+        LBM_STORAGE_DISPATCH(storage, T,
+                             k_wall_loads<27, T><<<grid, BLOCK, 0, s>>>(G, B, static_cast<const T*>(A), mask, alpha,
+                                                                         ports, apply_ports, cells, links, n_links,
+                                                                         out))
     }
     return cudaGetLastError();
 }

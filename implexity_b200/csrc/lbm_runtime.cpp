@@ -355,6 +355,10 @@ struct lbm_handle {
     int64_t peak_extra = 0;  // second-level checkpoint bytes of the last horizon gradient
     std::vector<Checkpoint> ckpts;
     std::vector<StepDiag> last_trajectory;
+    // fixed-wall links of the momentum-exchange loads (wall_exchange.rs layout)
+    std::vector<uint32_t> wall_cells;
+    std::vector<uint8_t> wall_links;
+    DevBuf wall_cells_d, wall_links_d, wall_out;
     // --- state
     bool design_set = false, state_valid = false, forward_done = false;
     int cur = 0;   // which population array holds the current state
@@ -685,6 +689,23 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
     }
     for (size_t k = 0; k < port_cells.size(); ++k)
         for (int64_t x : port_cells[k]) mask[x] |= (uint32_t)(k + 1) << MASK_PORT_SHIFT;
+
+    // wall links of the momentum-exchange loads (wall_exchange.rs:44-70): every
+    // blocked pull link of a fluid cell, cells and links in order, except the
+    // links of a port cell that point along its port's inward normal
+    h.wall_cells.clear();
+    h.wall_links.clear();
+    for (int64_t x = 0; x < n; ++x) {
+        const uint32_t m = mask[x];
+        if (m & MASK_SOLID) continue;
+        const int port = (int)((m >> MASK_PORT_SHIFT) & 7u) - 1;
+        for (int q = 0; q < h.Q; ++q) {
+            if (!((m >> q) & 1u)) continue;
+            if (port >= 0 && h.L.c[q][specs[port].axis] == specs[port].sign) continue;
+            h.wall_cells.push_back((uint32_t)x);
+            h.wall_links.push_back((uint8_t)q);
+        }
+    }
 
     // design map (design.rs:109-171); box filter is the documented extension
     h.cls.assign(n, 0);
@@ -1842,6 +1863,59 @@ lbm_status lbm_responses(lbm_handle* h, double* out8) {
         if (!h->state_valid) throw StateError("no current state");
         require_design(*h);
         responses(*h, out8, nullptr);
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_wall_loads(lbm_handle* h, double pressure_datum_pa, const double* origin_m, double* positions_m,
+                          double* force_n, size_t capacity, size_t* n_links) {
+    return guarded(h, [&]() {
+        const size_t nl = h->wall_cells.size();
+        if (n_links) *n_links = nl;
+        if (!positions_m && !force_n) return LBM_OK;
+        if (capacity < nl) throw ContractError("wall load outputs need room for n_links links");
+        if (!std::isfinite(pressure_datum_pa)) throw ContractError("pressure datum must be finite");
+        const double org[3] = {origin_m ? origin_m[0] : 0.0, origin_m ? origin_m[1] : 0.0,
+                               origin_m ? origin_m[2] : 0.0};
+        if (positions_m)
+            for (size_t i = 0; i < nl; ++i) {
+                const int64_t x = h->wall_cells[i];
+                const int q = h->wall_links[i];
+                const int64_t c[3] = {x / h->G.sx, (x / h->G.sy) % h->G.ny, x % h->G.nz};
+                for (int a = 0; a < 3; ++a)
+                    positions_m[3 * i + a] = org[a] + ((double)c[a] + 0.5 - 0.5 * h->L.c[q][a]) * h->dx;
+            }
+        if (!force_n) return LBM_OK;
+        if (!h->forward_done || !h->state_valid || h->t < 1)
+            throw StateError("wall loads need the states of a successful lbm_forward");
+        require_design(*h);
+        int64_t* ctr = &h->device_bytes;
+        if (nl > 0) {
+            h->wall_cells_d.alloc(nl * sizeof(uint32_t), ctr);
+            h->wall_links_d.alloc(nl, ctr);
+            h->wall_out.alloc(nl * sizeof(double), ctr);
+            CK(cudaMemcpyAsync(h->wall_cells_d.p, h->wall_cells.data(), nl * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                               h->stream));
+            CK(cudaMemcpyAsync(h->wall_links_d.p, h->wall_links.data(), nl, cudaMemcpyHostToDevice, h->stream));
+            // the state before the last step, pulled from the previous array
+            const int64_t tb = h->t - 1;
+            const void* prev = h->pop_array(h->cur ^ 1) + pop_pad(h->G) * storage_bytes(h->storage);
+            CK(launch_wall_loads(h->Q, h->storage, h->G, h->P, prev, h->mask.as<uint32_t>(), h->alpha.as<float>(),
+                                 ports_at(*h, tb), (tb >= 1 && h->n_ports > 0) ? 1 : 0, h->wall_cells_d.as<uint32_t>(),
+                                 h->wall_links_d.as<uint8_t>(), (int64_t)nl, h->wall_out.as<double>(), h->stream));
+        }
+        std::vector<double> g(nl);
+        if (nl > 0) CK(cudaMemcpyAsync(g.data(), h->wall_out.p, nl * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        // loads_from_post (wall_exchange.rs:86-100) in shifted populations:
+        // f*_opp - w_q + w_q datum / unit = g*_opp + w_q datum / unit
+        const double scale = h->density * std::pow(h->dx, 4) / (h->dt * h->dt);
+        const double unit = h->density * (h->dx / h->dt) * (h->dx / h->dt) / 3.0;
+        for (size_t i = 0; i < nl; ++i) {
+            const int q = h->wall_links[i];
+            const double mag = g[i] + h->L.w[q] * pressure_datum_pa / unit;
+            for (int a = 0; a < 3; ++a) force_n[3 * i + a] = -2.0 * h->L.c[q][a] * mag * scale;
+        }
         return LBM_OK;
     });
 }

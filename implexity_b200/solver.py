@@ -210,6 +210,19 @@ class LbmSolver:
         self._check(self.lib.lbm_responses(self.h, _dp(out)))
         return out
 
+    def wall_loads(self, pressure_datum_pa: float = 0.0) -> dict[str, np.ndarray]:
+        """Fixed-wall momentum-exchange loads of the last interval: link
+        midpoints [n,3] (m) and forces [n,3] (N), as evaluate_value's
+        wall_link_positions_m / wall_link_gauge_force_N."""
+        n = C.c_size_t(0)
+        self._check(self.lib.lbm_wall_loads(self.h, 0.0, None, None, None, 0, C.byref(n)))
+        pos = np.empty((n.value, 3))
+        force = np.empty((n.value, 3))
+        origin = np.ascontiguousarray(self.problem.origin_m, dtype=np.float64)
+        self._check(self.lib.lbm_wall_loads(self.h, float(pressure_datum_pa), _dp(origin), _dp(pos), _dp(force),
+                                            n.value, C.byref(n)))
+        return {"wall_link_positions_m": pos, "wall_link_gauge_force_N": force}
+
     def fields(self) -> dict[str, np.ndarray]:
         rho = np.empty(self.shape)
         vel = np.empty(tuple(self.shape) + (3,))

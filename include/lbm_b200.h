@@ -314,6 +314,20 @@ LBM_API lbm_status lbm_responses(lbm_handle* h, double* out8);
  * engine's samples, restated). */
 LBM_API lbm_status lbm_time_average(lbm_handle* h, double* out8);
 
+/* Fixed-wall momentum-exchange loads of the last interval
+ * (wall_exchange::loads, wall_exchange.rs:79-100, as evaluate_value reports
+ * them, provider.rs:312-321): one entry per blocked pull link of a fluid cell
+ * (cells and links in order; a port cell's links along its port's inward
+ * normal are not walls, wall_exchange.rs:44-70).  The state before the last
+ * step is collided with the Guo-BGK collision (solver::collide, whatever the
+ * problem's collision, as the reference does) and the force on the link is
+ * -2 c_q (f*_opp(q) - w_q + w_q datum / (rho c^2 / 3)) rho dx^4 / dt^2 [N].
+ * positions_m [n,3] are the link midpoints plus origin_m (NULL: 0);
+ * force_n [n,3].  n_links receives the count; with both outputs NULL only the
+ * count is returned, otherwise they need capacity >= n_links entries. */
+LBM_API lbm_status lbm_wall_loads(lbm_handle* h, double pressure_datum_pa, const double* origin_m,
+                                  double* positions_m, double* force_n, size_t capacity, size_t* n_links);
+
 /* Physical fields of the current state (LbmProblem::fields, provider.rs
  * flow_fields): density [N] kg/m^3, velocity [N*3] m/s, gauge pressure [N] Pa.
  * Any pointer may be NULL. */

@@ -1331,6 +1331,44 @@ void orc_interval_vjp(const orc_problem* o, const double* before, const double* 
 
 void orc_set_time(const orc_problem* o, int64_t t_index) { set_port_time(*o, t_index); }
 
+// Fixed-wall momentum-exchange loads (wall_exchange.rs: layout :44-70, loads
+// :79-84, loads_from_post :86-100): `before` is collided with the Guo-BGK
+// collision; for every blocked pull link q of a fluid cell (cells, then
+// links, in order) that is not a port cell's link along its port's inward
+// normal, force = -2 c_q (post_opp(q) - w_q + w_q datum / unit) scale.
+// Returns the number of links; forces (3 per link) when not NULL.
+int64_t orc_wall_loads(const orc_problem* o, const double* before, const double* alpha, double datum_pa,
+                       double* forces) {
+    const int Q = o->Q;
+    const Lattice& L = o->L;
+    std::vector<int> port_of(o->N, -1);
+    for (size_t k = 0; k < o->ports.size(); ++k)
+        for (int64_t x : o->ports[k].cells) port_of[x] = (int)k;
+    const double scale = o->density * std::pow(o->dx, 4) / (o->dt * o->dt);
+    const double unit = o->density * (o->dx / o->dt) * (o->dx / o->dt) / 3.0;
+    int64_t n = 0;
+    std::vector<double> post(Q);
+    for (int64_t x = 0; x < o->N; ++x) {
+        if (o->solid[x]) continue;
+        bool collided = false;
+        for (int q = 0; q < Q; ++q) {
+            if (!o->blocked[x * Q + q]) continue;
+            const int k = port_of[x];
+            if (k >= 0 && L.c[q][o->ports[k].axis] == o->ports[k].sign) continue;
+            if (forces) {
+                if (!collided) {
+                    collide_bgk(*o, before + x * Q, alpha[x], post.data());
+                    collided = true;
+                }
+                const double mag = post[L.opp[q]] - L.w[q] + L.w[q] * datum_pa / unit;
+                for (int a = 0; a < 3; ++a) forces[3 * n + a] = -2.0 * L.c[q][a] * mag * scale;
+            }
+            ++n;
+        }
+    }
+    return n;
+}
+
 void orc_port_apply(const orc_problem* o, int port, const double* f_in, double* f_out) {
     reconstruct(*o, o->ports[port], f_in, f_out);
 }

@@ -84,6 +84,8 @@ def lib() -> C.CDLL:
         L.orc_mrt_basis.argtypes = [C.c_int, _dp, _dp, C.POINTER(C.c_int32)]
         L.orc_set_time.argtypes = [h, C.c_int64]
         L.orc_set_time.restype = None
+        L.orc_wall_loads.argtypes = [h, _dp, _dp, C.c_double, _dp]
+        L.orc_wall_loads.restype = C.c_int64
         L.orc_port_apply.argtypes = [h, C.c_int, _dp, _dp]
         L.orc_port_apply.restype = None
         _lib = L
@@ -217,6 +219,15 @@ class Oracle:
         st = lib().orc_gradient(self.h, _p(raw), _p(w8), int(steps), m, int(K),
                                 float(tol), int(max_iter), _p(grad), _p(resp), C.byref(rep))
         return grad, resp, rep, st
+
+    def wall_loads(self, before, alpha, pressure_datum_pa=0.0):
+        """Wall momentum-exchange forces [n,3] (N) of the interval starting at `before`."""
+        b = np.ascontiguousarray(before, dtype=np.float64).reshape(-1)
+        al = np.ascontiguousarray(alpha, dtype=np.float64)
+        n = lib().orc_wall_loads(self.h, _p(b), _p(al), float(pressure_datum_pa), None)
+        out = np.empty((n, 3))
+        lib().orc_wall_loads(self.h, _p(b), _p(al), float(pressure_datum_pa), _p(out))
+        return out
 
     def set_time(self, t_index: int):
         """Port values of the reconstruction producing state t_index."""

@@ -308,3 +308,40 @@ def test_bounded_wait_runs_out_and_the_context_stays_usable(gpu_lib):
         s.set_design(raw)
         d = s.forward()
         assert d.admitted
+
+
+@pytest.mark.parametrize("lattice,coll,storage", [("D3Q19", "trt", "float32"), ("D3Q27", "trt", "float32"),
+                                                  ("D3Q19", "bgk", "float32"), ("D3Q19", "trt", "float16")])
+def test_wall_loads_match_oracle(gpu_lib, lattice, coll, storage):
+    """Momentum-exchange loads of the last interval (wall_exchange.rs): every
+    blocked link of walls and solids except the port faces, from the state
+    before the last step collided with Guo-BGK."""
+    shape = (14, 9, 8)
+    solid = np.zeros(shape, bool)
+    solid[4:6, 0:3, 0:2] = True
+    solid[8, 4, 3:8] = True
+    solid[1, 2, 2] = True
+    steps = 40
+    prob = workloads.channel_problem(shape=shape, steps=steps, collision=coll, lattice=lattice, storage=storage,
+                                     solid=solid)
+    prob["origin_m"] = [0.01, -0.02, 0.003]
+    norm = normalize(prob)
+    raw = workloads.uniform_design(shape, 3)
+    o = Oracle(norm)
+    _, alpha = o.design(raw)
+    before, _ = o.history(alpha, steps - 1)
+    datum = 12.5
+    f_ref = o.wall_loads(before, alpha, datum)
+    with LbmSolver(prob) as s:
+        s.set_design(raw)
+        s.forward()
+        loads = s.wall_loads(datum)
+    pos, force = loads["wall_link_positions_m"], loads["wall_link_gauge_force_N"]
+    assert force.shape == f_ref.shape and len(force) > 0
+    tol = 1e-5 if storage == "float32" else 2e-3
+    assert np.max(np.abs(force - f_ref)) <= tol * np.max(np.abs(f_ref))
+    # link midpoints: origin + (ijk + 1/2 - c_q / 2) dx, links in (cell, q) order
+    assert np.all(np.isfinite(pos))
+    dx = norm.spacing_m
+    ijk = np.rint((pos - np.array(prob["origin_m"])) / dx - 0.5)
+    assert np.all(np.abs((pos - np.array(prob["origin_m"])) / dx - 0.5 - ijk) <= 0.5 + 1e-9)
