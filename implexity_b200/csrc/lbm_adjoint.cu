@@ -82,6 +82,8 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
         const int c = threadIdx.x - 32;
         int s = 0;
         uint32_t round = 0;
+        const float s_in = 1.f / a.in_scale_inv;        // stored scale of the input
+        const float k_out = a.out_scale * a.in_scale_inv;  // stored input -> stored output
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
             const uint32_t x = tile * TILE + c;
             // the running alpha cotangent, read before the wait so that its
@@ -103,17 +105,17 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
                         for (int q = 1; q < Q; ++q)
                             if ((m >> opp<Q>(q)) & 1u) v[q] = Cvt<T>::to(B[opp<Q>(q) * n + x]);
                     }
-#pragma unroll
-                    for (int q = 0; q < Q; ++q) v[q] *= a.in_scale_inv;
                 } else {
 #pragma unroll
-                    for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(B[pull_adj_index<Q>(a.G, x, m, q)]) * a.in_scale_inv;
+                    for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(B[pull_adj_index<Q>(a.G, x, m, q)]);
                 }
             }
             if (fluid) {
                 const float u[3] = {st->rec[1][a.recd[1] + c], st->rec[2][a.recd[2] + c], st->rec[3][a.recd[3] + c]};
                 const float rp = st->rec[0][a.recd[0] + c];
-                float ab = collide_vjp<Q, COLL>(v, rp, u, st->alpha[c], a.P);
+                // v stays in the stored scale (the transposed step is linear): the
+                // alpha cotangent is rescaled once, the output by out_scale / in_scale
+                float ab = collide_vjp<Q, COLL>(v, rp, u, st->alpha[c], a.P) * a.in_scale_inv;
                 if constexpr (STG) {
                     if (a.stage) {
                         // the stage seed of this state: d(w . responses)/dg from its record
@@ -124,16 +126,16 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
                         ab += response_vjp<Q>(rp, u, Sm, st->alpha[c], pm ? pm->dp_weight : 0.f, pm != nullptr, a.seed,
                                               a.P, fb);
 #pragma unroll
-                        for (int q = 0; q < Q; ++q) v[q] += fb[q];
+                        for (int q = 0; q < Q; ++q) v[q] = fmaf(fb[q], s_in, v[q]);
                     }
                 }
                 a.abar[x] = fmaf(ab, a.abar_factor, ab_prev);
                 if (a.port_transpose && (m & MASK_PORT)) port_transpose<Q>(a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], v);
-                store_own_lam<Q, T>(D, n, x, v, a.out_scale);
+                store_own_lam<Q, T>(D, n, x, v, k_out);
                 if (a.norm2) {
 #pragma unroll
                     for (int q = 0; q < Q; ++q) {
-                        const float sv = v[q] * a.out_scale;
+                        const float sv = v[q] * k_out;
                         nsum += (double)sv * (double)sv;
                     }
                 }
