@@ -380,11 +380,29 @@ __device__ __forceinline__ Macro collide_fused(float (&v)[Q], float alpha, const
         const float E0 = fmaf(om, fmaf(-rho, usq15, rp), -kp * uf3);
         const float A = 4.5f * om * rho, G = 3.f * omm * rho;
         const float K9 = 9.f * kp, K3 = 3.f * km;
+        // MRT_BULK: the bulk moment Eb = sum_i w_i b_i y_i of y = f - eq + src/2,
+        // b_i = |c_i|^2 - 1 (zero on the axis directions); per pair
+        // y_p = S/2 - w [e0 + 4.5 cu (rho cu - cf)], e0 = rp - 1.5 rho u^2 + 1.5 u.F
+        float Eb = 0.f, e0 = 0.f;
+        if constexpr (COLL == CK_MRT_BULK) {
+            const float w0 = SC ? 1.f : L::w(0);
+            const float y0 = v[0] - w0 * (rp - rho * usq15) - 0.5f * w0 * uf3;
+            Eb = -(SC ? L::w(0) : 1.f) * y0;
+            e0 = fmaf(-rho, usq15, rp) + 0.5f * uf3;
+        }
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
             const int i = k + 1, o = opp<Q>(i);
             const float cu = dotc<Q>(i, M.u);
             const float cf = dotc<Q>(i, M.F);
+            if constexpr (COLL == CK_MRT_BULK) {
+                const int c2 = L::cx(i) * L::cx(i) + L::cy(i) * L::cy(i) + L::cz(i) * L::cz(i);
+                if (c2 != 1) {  // folded after unrolling
+                    const float wy = SC ? 1.f : L::w(i);
+                    const float yp = fmaf(-wy, fmaf(4.5f * cu, fmaf(rho, cu, -cf), e0), 0.5f * S[k]);
+                    Eb = fmaf((SC ? 2.f * L::w(i) : 2.f) * (float)(c2 - 1), yp, Eb);
+                }
+            }
             const float tp = fmaf(cu * cf, K9, fmaf(cu * cu, A, E0));
             const float tm = fmaf(cu, G, cf * K3);
             float Pp, Dm;
@@ -398,6 +416,22 @@ __device__ __forceinline__ Macro collide_fused(float (&v)[Q], float alpha, const
             v[i] = Pp + Dm;
             v[o] = Pp - Dm;
             rem = fmaf(SC ? -2.f * L::w(i) : -2.f, Pp, rem);
+        }
+        if constexpr (COLL == CK_MRT_BULK) {
+            // rank-one bulk correction: v_i -= (s_bulk - omega) Eb w_i b_i / |b|^2_W,
+            // |b|^2_W = 2/3 on both lattices; the rest population keeps the mass
+            const float cb = P.proj_rate[0] * Eb * 1.5f;
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                const int i = k + 1, o = opp<Q>(i);
+                const int c2 = L::cx(i) * L::cx(i) + L::cy(i) * L::cy(i) + L::cz(i) * L::cz(i);
+                if (c2 != 1) {  // folded after unrolling
+                    const float dv = cb * (float)(c2 - 1) * (SC ? 1.f : L::w(i));
+                    v[i] -= dv;
+                    v[o] -= dv;
+                    rem = fmaf(SC ? 2.f * L::w(i) : 2.f, dv, rem);
+                }
+            }
         }
     } else {
 #pragma unroll

@@ -290,12 +290,16 @@ cudaError_t launch_forward(int Q, int coll, int storage, const FwdArgs& a0, int 
     if (Q == 19) {
         if (coll == CK_MRT) {
             LBM_STORAGE_DISPATCH(storage, T, return run_forward<19, CK_MRT, T>(a, s))
+        } else if (coll == CK_MRT_BULK) {
+            LBM_STORAGE_DISPATCH(storage, T, return run_forward<19, CK_MRT_BULK, T>(a, s))
         } else {
             LBM_STORAGE_DISPATCH(storage, T, return run_forward<19, CK_PAIRS, T>(a, s))
         }
     } else {
         if (coll == CK_MRT) {
             LBM_STORAGE_DISPATCH(storage, T, return run_forward<27, CK_MRT, T>(a, s))
+        } else if (coll == CK_MRT_BULK) {
+            LBM_STORAGE_DISPATCH(storage, T, return run_forward<27, CK_MRT_BULK, T>(a, s))
         } else {
             LBM_STORAGE_DISPATCH(storage, T, return run_forward<27, CK_PAIRS, T>(a, s))
         }

@@ -17,7 +17,9 @@ namespace lbm {
 constexpr int64_t CELL_PAD = 1024;
 inline int64_t pop_pad(const Geometry& G) { return ((G.sx + G.sy + 1 + 2 * CELL_PAD) + 63) / 64 * 64; }
 enum StoreKind { ST_F32 = 0, ST_F16 = 1, ST_BF16 = 2 };
-enum CollKind { CK_PAIRS = 0, CK_MRT = 1 };  // BGK runs as PAIRS with om == omega
+// BGK runs as PAIRS with om == omega; MRT_BULK is MRT whose only correction is
+// the bulk moment of the Gram-Schmidt basis (b = |c|^2 - 1), folded at compile time
+enum CollKind { CK_PAIRS = 0, CK_MRT = 1, CK_MRT_BULK = 2 };
 
 struct FwdArgs {
     Geometry G;

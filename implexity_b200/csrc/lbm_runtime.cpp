@@ -355,6 +355,7 @@ struct lbm_handle {
     int64_t peak_extra = 0;  // second-level checkpoint bytes of the last horizon gradient
     std::vector<Checkpoint> ckpts;
     std::vector<StepDiag> last_trajectory;
+    bool bulk_only = false;  // MRT: the single correction is the bulk moment |c|^2 - 1
     // fixed-wall links of the momentum-exchange loads (wall_exchange.rs layout)
     std::vector<uint32_t> wall_cells;
     std::vector<uint8_t> wall_links;
@@ -540,6 +541,7 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
     h.P.om = (float)h.om;
     for (int d = 0; d < 3; ++d) h.P.a[d] = (float)h.a[d];
     h.P.n_proj = 0;
+    h.bulk_only = false;
     if (p.collision == LBM_MRT) {
         std::vector<std::vector<double>> rows;
         std::vector<double> norms;
@@ -553,6 +555,14 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
             if (rate == h.omega) continue;
             int j = h.P.n_proj++;
             h.P.proj_rate[j] = (float)(rate - h.omega);
+            // the bulk row is |c|^2 - 1 with |b|^2_W = 2/3: the forward step can
+            // fold it at compile time when it is the only correction
+            bool bulk_row = groups[k] == 2 && std::fabs(norms[k] - 2.0 / 3.0) < 1e-12;
+            for (int i = 0; i < h.Q; ++i) {
+                const int c2 = h.L.c[i][0] * h.L.c[i][0] + h.L.c[i][1] * h.L.c[i][1] + h.L.c[i][2] * h.L.c[i][2];
+                bulk_row = bulk_row && std::fabs(rows[k][i] - (c2 - 1.0)) < 1e-12;
+            }
+            h.bulk_only = (j == 0) && bulk_row;
             for (int i = 0; i < h.Q; ++i) {
                 h.P.proj_left[j][i] = (float)(h.L.w[i] * rows[k][i] / norms[k]);
                 h.P.proj_right[j][i] = (float)rows[k][i];
@@ -823,6 +833,12 @@ FwdArgs fwd_args(lbm_handle& h) {
 }
 
 int coll_kind(const lbm_handle& h) { return h.coll == LBM_MRT ? CK_MRT : CK_PAIRS; }
+// The forward step's collision kernel: MRT whose only correction is the bulk
+// moment runs the compile-time folded branch.
+int fwd_coll_kind(const lbm_handle& h) {
+    if (h.coll != LBM_MRT) return CK_PAIRS;
+    return (h.P.n_proj == 1 && h.bulk_only) ? CK_MRT_BULK : CK_MRT;
+}
 
 // One step of the current state; diag / record / the current state's
 // response sums (16 doubles) optional.
@@ -835,7 +851,7 @@ void step(lbm_handle& h, StepDiag* diag, float* record, bool record_s = false, d
     a.record_s = record_s ? 1 : 0;
     a.collide = 1;
     a.step = (uint32_t)h.t;
-    CK(launch_forward(h.Q, coll_kind(h), h.storage, a, grid_for(h), h.stream));
+    CK(launch_forward(h.Q, fwd_coll_kind(h), h.storage, a, grid_for(h), h.stream));
     h.cur ^= 1;
     h.restored = nullptr;
     h.pending = h.n_ports > 0;
@@ -852,7 +868,7 @@ void inspect(lbm_handle& h, StepDiag* diag, float* record, bool record_s = false
     a.record = record;
     a.record_s = record_s ? 1 : 0;
     a.collide = 0;
-    CK(launch_forward(h.Q, coll_kind(h), h.storage, a, grid_for(h), h.stream));
+    CK(launch_forward(h.Q, fwd_coll_kind(h), h.storage, a, grid_for(h), h.stream));
 }
 
 void init_state(lbm_handle& h) {

@@ -345,3 +345,26 @@ def test_wall_loads_match_oracle(gpu_lib, lattice, coll, storage):
     dx = norm.spacing_m
     ijk = np.rint((pos - np.array(prob["origin_m"])) / dx - 0.5)
     assert np.all(np.abs((pos - np.array(prob["origin_m"])) / dx - 0.5 - ijk) <= 0.5 + 1e-9)
+
+
+@pytest.mark.parametrize("lattice", ["D3Q19", "D3Q27"])
+def test_mrt_with_even_rate_matches_oracle(gpu_lib, lattice):
+    """MRT with a bulk and an even-high rate (two rank-one corrections: the
+    general branch; a bulk rate alone takes the compile-time folded one)."""
+    prob = workloads.channel_problem(shape=(16, 10, 8), steps=60, collision="mrt", lattice=lattice, mrt_bulk_rate=1.2)
+    prob["solver_options"]["collision"]["even_rate"] = 1.1
+    norm = normalize(prob)
+    raw = workloads.uniform_design(norm.shape, 1)
+    o = Oracle(norm)
+    _, alpha = o.design(raw)
+    f_ref, _ = o.history(alpha, 60)
+    w = workloads.objective_weights()
+    g_ref, _, _, st = o.gradient(raw, w, mode="horizon", K=12)
+    assert st == 0
+    with LbmSolver(norm) as s:
+        s.set_design(raw)
+        s.forward()
+        f = s.populations()
+        g, _ = s.gradient(w, mode="horizon", checkpoint_every=12)
+    assert rel_max(f, f_ref) < 1e-5
+    assert rel_l2(g, g_ref) < 1e-4, rel_l2(g, g_ref)
