@@ -207,12 +207,16 @@ cudaError_t launch_adjoint(int Q, int coll, int lstorage, const AdjArgs& a0, int
     if (Q == 19) {
         if (coll == CK_MRT) {
             LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint<19, CK_MRT, T>(a, s))
+        } else if (coll == CK_MRT_BULK) {
+            LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint<19, CK_MRT_BULK, T>(a, s))
         } else {
             LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint<19, CK_PAIRS, T>(a, s))
         }
     } else {
         if (coll == CK_MRT) {
             LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint<27, CK_MRT, T>(a, s))
+        } else if (coll == CK_MRT_BULK) {
+            LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint<27, CK_MRT_BULK, T>(a, s))
         } else {
             LBM_STORAGE_DISPATCH(lstorage, T, return run_adjoint<27, CK_PAIRS, T>(a, s))
         }

@@ -540,6 +540,33 @@ __device__ __forceinline__ float collide_vjp(float (&gb)[Q], float rp, const flo
         Z2[e] = om * M2[e];
         H2[e] = (1.f - 0.5f * om) * M2[e];
     }
+    if constexpr (COLL == CK_MRT_BULK) {
+        // the bulk correction folded: b_i = |c_i|^2 - 1, |b|^2_W = 2/3,
+        // sum_i w_i b_i = 0 and sum_i w_i b_i c_ia c_ib = 2/9 delta_ab on both lattices
+        float e = -L::w(0) * gb[0];
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            const int i = k + 1, o = opp<Q>(i);
+            const int c2 = L::cx(i) * L::cx(i) + L::cy(i) * L::cy(i) + L::cz(i) * L::cz(i);
+            if (c2 != 1) e = fmaf(L::w(i) * (float)(c2 - 1), gb[i] + gb[o], e);  // folded after unrolling
+        }
+        const float c = P.proj_rate[0] * e * 1.5f;
+        z[0] -= c;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            const int i = k + 1, o = opp<Q>(i);
+            const int c2 = L::cx(i) * L::cx(i) + L::cy(i) * L::cy(i) + L::cz(i) * L::cz(i);
+            if (c2 != 1) {
+                z[i] = fmaf(c, (float)(c2 - 1), z[i]);
+                z[o] = fmaf(c, (float)(c2 - 1), z[o]);
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            Z2[d] = fmaf(c, 2.f / 9.f, Z2[d]);
+            H2[d] = fmaf(-0.5f * c, 2.f / 9.f, H2[d]);
+        }
+    }
     if constexpr (COLL == CK_MRT) {
 #pragma unroll
         for (int p = 0; p < MAX_PROJ; ++p) {

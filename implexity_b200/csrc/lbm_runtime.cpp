@@ -832,10 +832,9 @@ FwdArgs fwd_args(lbm_handle& h) {
     return a;
 }
 
-int coll_kind(const lbm_handle& h) { return h.coll == LBM_MRT ? CK_MRT : CK_PAIRS; }
-// The forward step's collision kernel: MRT whose only correction is the bulk
+// The stepping kernels' collision: MRT whose only correction is the bulk
 // moment runs the compile-time folded branch.
-int fwd_coll_kind(const lbm_handle& h) {
+int coll_kernel(const lbm_handle& h) {
     if (h.coll != LBM_MRT) return CK_PAIRS;
     return (h.P.n_proj == 1 && h.bulk_only) ? CK_MRT_BULK : CK_MRT;
 }
@@ -851,7 +850,7 @@ void step(lbm_handle& h, StepDiag* diag, float* record, bool record_s = false, d
     a.record_s = record_s ? 1 : 0;
     a.collide = 1;
     a.step = (uint32_t)h.t;
-    CK(launch_forward(h.Q, fwd_coll_kind(h), h.storage, a, grid_for(h), h.stream));
+    CK(launch_forward(h.Q, coll_kernel(h), h.storage, a, grid_for(h), h.stream));
     h.cur ^= 1;
     h.restored = nullptr;
     h.pending = h.n_ports > 0;
@@ -868,7 +867,7 @@ void inspect(lbm_handle& h, StepDiag* diag, float* record, bool record_s = false
     a.record = record;
     a.record_s = record_s ? 1 : 0;
     a.collide = 0;
-    CK(launch_forward(h.Q, fwd_coll_kind(h), h.storage, a, grid_for(h), h.stream));
+    CK(launch_forward(h.Q, coll_kernel(h), h.storage, a, grid_for(h), h.stream));
 }
 
 void init_state(lbm_handle& h) {
@@ -1136,7 +1135,7 @@ void adjoint_step(lbm_handle& h, AdjState& st, const float* rec, bool want_norm,
     a.out_scale = st.target;
     a.abar_factor = st.s0;
     a.norm2 = want_norm ? h.norm2.as<double>() : nullptr;
-    CK(launch_adjoint(h.Q, coll_kind(h), h.lam_storage, a, grid_for(h), h.stream));
+    CK(launch_adjoint(h.Q, coll_kernel(h), h.lam_storage, a, grid_for(h), h.stream));
     h.lcur ^= 1;
     st.scale = st.target;
     st.first = false;
@@ -2073,7 +2072,7 @@ lbm_status lbm_step_vjp(lbm_handle* h, const double* state, const double* lambda
         a.in_scale_inv = 1.f;
         a.out_scale = 1.f;
         a.abar_factor = 1.f;
-        CK(launch_adjoint(Q, coll_kind(*h), LBM_STORE_F32, a, grid_for(*h), h->stream));
+        CK(launch_adjoint(Q, coll_kernel(*h), LBM_STORE_F32, a, grid_for(*h), h->stream));
         h->lcur ^= 1;
         check_errflag(*h);
         CK(launch_canon_lam(Q, LBM_STORE_F32, h->G, h->lamA(), h->mask.as<uint32_t>(), 1.f, h->scratch.as<float>(),
