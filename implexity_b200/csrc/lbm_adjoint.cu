@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
     constexpr int NREC = STG ? 10 : 4;
     using S = AdjStage<Q, T, NREC>;
     constexpr int NCOPY = Q + NREC + 2;  // runs of lambda, the record, mask and alpha
-    constexpr int STAGES = Ring<T>::STAGES;
+    constexpr int STAGES = ring_depth<S, T>();
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);  // stage loaded
     uint64_t* empty = full + STAGES;                      // stage consumed
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
 
 template <int Q, int COLL, typename T, int AL, int STG>
 cudaError_t run_adjoint_al(const AdjArgs& a, cudaStream_t s) {
-    constexpr size_t smem = pipe_bytes<AdjStage<Q, T, STG ? 10 : 4>, Ring<T>::STAGES>();
+    constexpr size_t smem = pipe_bytes<AdjStage<Q, T, STG ? 10 : 4>, ring_depth<AdjStage<Q, T, STG ? 10 : 4>, T>()>();
     static bool attr = false;
     if (!attr) {
         cudaError_t e = set_smem(k_adjoint<Q, COLL, T, AL, STG>, smem);

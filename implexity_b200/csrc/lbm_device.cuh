@@ -1102,6 +1102,13 @@ template <typename S, int NS>
 __host__ __device__ constexpr size_t pipe_bytes() {
     return PIPE_HEAD + NS * stage_stride<S>();
 }
+// Ring depth of a stage type: the storage width's depth, reduced to two
+// stages where the deeper ring would leave room for only one block per SM
+// (half of the 227 KB a block may use, less the static reduction scratch).
+template <typename S, typename T>
+__host__ __device__ constexpr int ring_depth() {
+    return (Ring<T>::STAGES > 2 && pipe_bytes<S, Ring<T>::STAGES>() > 105 * 1024) ? 2 : Ring<T>::STAGES;
+}
 template <typename S>
 __device__ __forceinline__ S* stage_at(unsigned char* smem, int s) {
     return reinterpret_cast<S*>(smem + PIPE_HEAD + s * stage_stride<S>());

@@ -28,7 +28,7 @@ template <int Q, int COLL, typename T, int AL, int RSP>
 __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
     using L = Lat<Q>;
     using S = FwdStage<Q, T>;
-    constexpr int STAGES = Ring<T>::STAGES;
+    constexpr int STAGES = ring_depth<S, T>();
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);  // stage loaded
     uint64_t* empty = full + STAGES;                      // stage consumed (outputs written into it)
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
 
 template <int Q, int COLL, typename T, int AL, int RSP>
 cudaError_t run_forward_rs(const FwdArgs& a, cudaStream_t s) {
-    constexpr size_t smem = pipe_bytes<FwdStage<Q, T>, Ring<T>::STAGES>();
+    constexpr size_t smem = pipe_bytes<FwdStage<Q, T>, ring_depth<FwdStage<Q, T>, T>()>();
     static bool attr = false;
     if (!attr) {
         cudaError_t e = set_smem(k_forward<Q, COLL, T, AL, RSP>, smem);
