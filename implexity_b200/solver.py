@@ -51,6 +51,12 @@ def _raise(status: int, msg: str):
     raise cls(msg)
 
 
+def _choice(name: str, value: str, table: dict) -> int:
+    if value not in table:
+        raise ContractError(f"{name} must be one of {', '.join(table)} (got {value!r})")
+    return table[value]
+
+
 def _dp(a: np.ndarray | None):
     if a is None:
         return None
@@ -253,15 +259,17 @@ class LbmSolver:
         w = np.zeros(_abi.N_RESPONSES)
         w[: len(weights)] = np.asarray(weights, dtype=float)
         o = _abi.AdjointOpts()
-        o.mode = _abi.LBM_ADJ_STEADY if mode == "steady" else _abi.LBM_ADJ_HORIZON
-        o.lambda_storage = {"float32": 0, "float16": 1, "bfloat16": 2}[lambda_storage]
+        o.mode = _choice("mode", mode, {"horizon": _abi.LBM_ADJ_HORIZON, "steady": _abi.LBM_ADJ_STEADY})
+        o.lambda_storage = _choice("lambda_storage", lambda_storage, {"float32": 0, "float16": 1, "bfloat16": 2})
         o.checkpoint_every = int(checkpoint_every)
         o.max_iterations = int(max_iterations)
         o.check_every = int(check_every)
         o.tolerance = float(tolerance)
         o.record_budget_bytes = int(record_budget_bytes)
-        o.objective = {"final": _abi.LBM_OBJ_FINAL, "time_average": _abi.LBM_OBJ_TIME_AVERAGE}[objective]
-        o.checkpointing = {"every": _abi.LBM_CKPT_EVERY, "binomial": _abi.LBM_CKPT_BINOMIAL}[checkpointing]
+        o.objective = _choice("objective", objective,
+                              {"final": _abi.LBM_OBJ_FINAL, "time_average": _abi.LBM_OBJ_TIME_AVERAGE})
+        o.checkpointing = _choice("checkpointing", checkpointing,
+                                  {"every": _abi.LBM_CKPT_EVERY, "binomial": _abi.LBM_CKPT_BINOMIAL})
         o.snapshots = int(snapshots)
         grad = np.empty(self.shape)
         rep = _abi.AdjointReport()

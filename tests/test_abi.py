@@ -168,3 +168,45 @@ def test_collision_parameters():
     p["solver_options"]["collision"] = {"kind": "cumulant"}
     with pytest.raises(ContractError, match="collision kind must be bgk, trt or mrt"):
         normalize(p)
+
+
+def test_ctypes_layouts_match_the_header(tmp_path):
+    """Every struct the Python mirrors pass through the C-ABIs (lbm_b200.h,
+    mma_cpu.h) has the size and field offsets that the C compiler gives the
+    header's declaration."""
+    import ctypes as C
+
+    from implexity_b200 import mma
+
+    structs = {"lbm_port_t": _abi.Port, "lbm_problem_t": _abi.Problem, "lbm_diag_t": _abi.Diag,
+               "lbm_adjoint_opts_t": _abi.AdjointOpts, "lbm_adjoint_report_t": _abi.AdjointReport,
+               "lbm_info_t": _abi.Info, "mma_options_t": mma.Options, "mma_info_t": mma.Info}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "lbm_b200.h"', '#include "mma_cpu.h"',
+             "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'    printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in py._fields_:
+            lines.append(f'    printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    cc = shutil.which("gcc") or "/usr/bin/gcc"
+    exe = tmp_path / "layout"
+    r = subprocess.run([cc, "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], capture_output=True,
+                       text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for field, _ in py._fields_:
+            assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
+
+
+def test_gradient_option_names_are_checked():
+    """Unknown option names fail as contract errors before any device call."""
+    from implexity_b200.solver import _choice
+
+    assert _choice("mode", "steady", {"horizon": 0, "steady": 1}) == 1
+    with pytest.raises(ContractError, match="checkpointing must be one of every, binomial"):
+        _choice("checkpointing", "revolve", {"every": 0, "binomial": 1})
