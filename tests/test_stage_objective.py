@@ -139,3 +139,21 @@ def test_two_level_checkpoints_match_one_level(gpu_lib):
                             record_budget_bytes=6 * rec_bytes)
     assert r2.forward_recomputed > r1.forward_recomputed
     assert rel_l2(g2, g1) < 1e-6
+
+
+@pytest.mark.gpu
+def test_unsteady_driver_reports_every_schedule(gpu_lib):
+    """The K-sweep driver on a small pulsatile grid: every schedule reports its
+    memory and recomputation, and all of them give the same gradient."""
+    from implexity_b200 import unsteady
+
+    logs = []
+    base, recs = unsteady.run((12, 8, 6), 40, [10, 40], period_steps=16, snapshots=(3,), log=logs.append)
+    assert base["objective_time_average"] > 0.0
+    assert [r.get("K", r.get("binomial_snapshots")) for r in recs] == [10, 40, 3]
+    for r in recs:
+        assert r["adjoint_steps"] == 40
+        assert r["peak_state_GB"] > 0.0
+        assert r["grad_rel_l2_vs_first_K"] < 1e-5
+    assert recs[2]["forward_recomputed"] > recs[0]["forward_recomputed"]
+    assert len(logs) == 1 + len(recs)
