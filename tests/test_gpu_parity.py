@@ -368,3 +368,23 @@ def test_mrt_with_even_rate_matches_oracle(gpu_lib, lattice):
         g, _ = s.gradient(w, mode="horizon", checkpoint_every=12)
     assert rel_max(f, f_ref) < 1e-5
     assert rel_l2(g, g_ref) < 1e-4, rel_l2(g, g_ref)
+
+
+def test_bf16_storage_close_to_fp32(gpu_lib):
+    """BF16 storage of (f - w)/w (8 mantissa bits): velocity and steady
+    gradient stay within the format's resolution of the FP32 run."""
+    prob32, norm, raw = make("trt", "D3Q19", steps=600)
+    prob16, _, _ = make("trt", "D3Q19", steps=600, storage="bfloat16")
+    w = workloads.objective_weights()
+    with LbmSolver(prob32) as s32, LbmSolver(prob16) as s16:
+        for s in (s32, s16):
+            s.set_design(raw)
+            s.forward()
+        f32, f16 = s32.populations(), s16.populations()
+        _, alpha = s32.design()
+        _, u32 = macroscopic(f32, 19, alpha.ravel(), s32.acceleration_lattice)
+        _, u16 = macroscopic(f16, 19, alpha.ravel(), s16.acceleration_lattice)
+        assert rel_max(u16, u32) < 2e-2, rel_max(u16, u32)
+        g32, _ = s32.gradient(w, mode="steady", tolerance=1e-8)
+        g16, _ = s16.gradient(w, mode="steady", tolerance=1e-8, lambda_storage="bfloat16")
+        assert rel_l2(g16, g32) < 1e-2, rel_l2(g16, g32)

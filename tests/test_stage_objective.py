@@ -157,3 +157,25 @@ def test_unsteady_driver_reports_every_schedule(gpu_lib):
         assert r["grad_rel_l2_vs_first_K"] < 1e-5
     assert recs[2]["forward_recomputed"] > recs[0]["forward_recomputed"]
     assert len(logs) == 1 + len(recs)
+
+
+@pytest.mark.gpu
+def test_fp16_time_average_close_to_fp32(gpu_lib):
+    """16-bit storage through the fused response sums and the stage adjoint:
+    time average and gradient within the format's resolution of FP32."""
+    out = {}
+    for storage in ("float32", "float16"):
+        prob = workloads.pulsatile_problem(shape=(10, 7, 6), steps=40, lattice="D3Q19", u_mean=0.04, amp_frac=0.5,
+                                           period_steps=16, ramp_steps=6, box_half_width=1, storage=storage)
+        raw = workloads.uniform_design((10, 7, 6), 2)
+        with LbmSolver(prob) as s:
+            s.set_design(raw)
+            s.forward()
+            avg = s.time_average()
+            g, _ = s.gradient(workloads.objective_weights(), mode="horizon", checkpoint_every=10,
+                              objective="time_average", lambda_storage=storage)
+        out[storage] = (avg, g)
+    (a32, g32), (a16, g16) = out["float32"], out["float16"]
+    for k in (3, 6, 7):
+        assert abs(a16[k] - a32[k]) <= 5e-3 * abs(a32[k]), (k, a16[k], a32[k])
+    assert rel_l2(g16, g32) < 5e-3, rel_l2(g16, g32)
