@@ -3,8 +3,8 @@
 //
 // Some callers cannot call cudaMalloc: code running inside another
 // framework's memory pool or arena (the pool owns every device allocation and
-// forbids out-of-band ones), code between the capture calls of a CUDA graph,
-// or embedded hosts that budget device memory up front.  They already hold
+// forbids out-of-band ones), or embedded hosts that budget device memory up
+// front.  They already hold
 // their populations on the device and only want the numbers the admission
 // check of LbmProblem::admit (solver.rs:708-793) computes for one state.
 // The reduction here is the same one the stepping kernels run every step

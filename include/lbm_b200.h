@@ -373,9 +373,8 @@ LBM_API lbm_status lbm_design_vjp(lbm_handle* h, const double* phi_bar, double* 
 
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory -- code inside another framework's memory pool or arena (the pool
- * owns all device memory), code that runs while a CUDA graph is being
- * captured, embedded hosts that fix their device budget up front -- and that
- * already hold a state on the device: the admission statistics of that one
+ * owns all device memory), embedded hosts that fix their device budget up
+ * front -- and that already hold a state on the device: the admission statistics of that one
  * state, computed by the same compensated reduction the stepping kernels run
  * every step (LbmProblem::admit quantities, solver.rs:714-755).
  *

@@ -1,7 +1,6 @@
 """lbm_state_stats_noalloc: admission statistics of a device-held state for
 callers that cannot allocate device memory (code inside another framework's
-memory pool, code running while a CUDA graph is captured, hosts with a fixed
-device budget).  The entry point keeps its scratch in a static device array,
+memory pool, hosts with a fixed device budget).  The entry point keeps its scratch in a static device array,
 so these callers pass only their own input and output buffers.
 
 Checked against the existing entry points: the per-state admission record of
