@@ -112,11 +112,18 @@ class LatticeBoltzmannProvider:
 
     def evaluate_value(self, problem, design) -> dict:
         s, _, diag = self.parts(problem, design)
+        # fixed-wall momentum exchange of the last interval (provider.rs:312-321)
+        loads = s.wall_loads(0.0)
+        diag["wall_load_convention"] = (
+            "Last interval fixed-wall momentum exchange, gauge datum zero; includes pressure and viscous effects, "
+            "not a solved structural coupling"
+        )
         values = s.responses()
         fields = s.fields()
         phi, _ = s.design()
         fields["fluid_fraction"] = phi
-        diag["wall_load_convention"] = "wall loads are not computed by the GPU provider"
+        if len(loads["wall_link_positions_m"]):  # insert_wall_fields (provider.rs:284-298)
+            fields.update(loads)
         return {
             "provider": NAME,
             "responses": {n: float(v) for n, v in zip(RESPONSES, values)},
