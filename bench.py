@@ -140,8 +140,6 @@ def barrier(world):
 
 
 def run_gpu(args, rank, world, local):
-    import ctypes
-
     import torch
 
     torch.cuda.set_device(local)

@@ -1,6 +1,5 @@
 """Shared fixtures.  GPU tests are marked ``gpu`` and run only on a B200 box
 (``pytest -m gpu``); everything else runs on CPU."""
-import os
 import sys
 from pathlib import Path
 
