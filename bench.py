@@ -1,18 +1,21 @@
 """Benchmark: MLUPS of one design iteration (forward + steady discrete adjoint +
 sensitivity) of the differentiable D3Q19 TRT lattice-Boltzmann channel.
 
-Workload (default): 128^3 cells, D3Q19 TRT (tau 0.8, magic 3/16), plug inlet
-u = 0.05, constant-density outlet, halfway bounce-back walls, seeded uniform
-design smoothed by a 3x3x3 box filter, RAMP q = 0.1 to alpha in [0, 0.1];
-5000 forward steps, then the steady adjoint to relative residual 1e-8 and the
-design-map transpose.  One bench "step" is one such design iteration.
+Workload (default): 256x128x128 cells, D3Q19 TRT (tau 0.8, magic 3/16), plug
+inlet u = 0.05, constant-density outlet, halfway bounce-back walls, seeded
+uniform design smoothed by a 3x3x3 box filter, RAMP q = 0.1 to alpha in
+[0, 0.1]; 3000 forward steps, then the steady adjoint to relative residual
+1e-8 and the design-map transpose.  One bench "step" is one such design
+iteration.  The 128^3 channel (5000 forward steps) and the MRT sphere
+workload run with --config.
 
 MLUPS = cells * (forward steps + adjoint iterations) / time / 1e6.
 ``value`` uses the device time of the stepping kernels (CUDA events on the
 library's stream, design resident in HBM); ``e2e`` is the wall time of the
 public API call sequence with the design uploaded from host memory and the
-gradient read back every step.  The population arrays (160 MB in FP32) exceed
-the 126 MB L2, so no explicit L2 flush is needed between steps.
+gradient read back every step.  The FP32 population arrays (320 MB at
+256x128x128, 160 MB at 128^3) exceed the 126 MB L2, so no explicit L2 flush
+is needed between steps.
 
 ``--impl reference`` times the CPU oracle (FP64 C++ restatement of the
 reference's Rust path, all host threads) on a bounded sample of the same
@@ -194,7 +197,7 @@ def run_gpu(args, rank, world, local):
         e2e = world * lups / wall / 1e6
         fwd_lups_per_s = cells * T * args.steps / (fwd_ms / 1e3)
         achieved = fwd_lups_per_s * fwd_b / 1e9
-        tag = f"k_forward_d3q{s.q}_{coll}_{storage}"
+        tag = f"k_forward_d3q{s.q}_{coll}_{storage}_{shape[0]}x{shape[1]}x{shape[2]}"
         traffic_cell = profiled_traffic(tag)
         results[variant] = {
             "value": value,
@@ -294,7 +297,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
-    ap.add_argument("--config", default="channel128_trt", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="channel256x128x128_trt", choices=sorted(CONFIGS))
     ap.add_argument("--variants", default="fp32,fp16")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--profile", action="store_true", help="run a short case of the bench kernels for ncu")

@@ -1,6 +1,6 @@
 // lbm_common.cuh -- lattice tables, cell-mask layout and kernel argument
-// blocks shared by the sm_100a kernels (lbm_kernels.cu) and the host runtime
-// (lbm_runtime.cpp).
+// blocks shared by the sm_100a kernels (lbm_forward.cu, lbm_adjoint.cu,
+// lbm_misc.cu, lbm_noalloc.cu) and the host runtime (lbm_runtime.cpp).
 #pragma once
 
 #include <cstdint>

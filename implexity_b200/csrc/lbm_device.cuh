@@ -1,28 +1,27 @@
 // lbm_device.cuh -- device building blocks shared by the sm_100a kernels
-// (lbm_forward.cu, lbm_adjoint.cu, lbm_misc.cu): storage conversions, AA-pattern
+// (lbm_forward.cu, lbm_adjoint.cu, lbm_misc.cu): storage conversions, pull
 // addressing, port maps, the collision and its transpose, compensated
 // reductions, and launch helpers.
 //
 // Memory layout (all on one GPU):
-//   populations  Q planes of n cells, plane q at pop + q*n; cells in the
-//                reference Grid order (i*ny + j)*nz + k, so axis 2 is the
-//                contiguous one.  FP32 stores g = f - w; FP16/BF16 store g/w.
+//   populations  two arrays (current, next), each Q planes of n cells, plane q
+//                at pop + q*n; cells in the reference Grid order
+//                (i*ny + j)*nz + k, so axis 2 is the contiguous one.  FP32
+//                stores g = f - w; FP16/BF16 store g/w.
 //   mask         one uint32 per cell (lbm_common.cuh)
 //   alpha, phi   FP32 per cell
-//   lambda       Q planes, adjoint populations (FP32/FP16/BF16, global scale)
+//   lambda       two arrays of Q planes, adjoint populations (FP32/FP16/BF16,
+//                global scale)
 //   record       4 FP32 planes (rho-1, u) of the forward state the adjoint
 //                linearises at
 //
-// Streaming is the AA pattern: one population array updated in place.  A step
-// of parity 0 reads a cell's own slots and writes its post-collision values
-// into the opposite slots of the same cell; a step of parity 1 reads the
-// neighbours' opposite slots (the post-collision values streaming in) and
-// writes to the neighbours' slots.  A blocked link (halfway bounce-back,
-// Streaming::new solver.rs:84-119) reads/writes the cell's own slot instead.
-// Every slot is read and written by exactly one thread per step, so the
-// update is race free without a second buffer.  The adjoint transposes the
-// same pattern: the AA scheme run with the velocities reversed (pull from
-// x + c_q), linearised at a recorded (rho, u).
+// Streaming is a pull between the two arrays (see pull_index below): a step
+// reads the post-collision populations streaming in from the neighbours of
+// the current array and writes the cell's own slots of the other one.  A
+// blocked link (halfway bounce-back, Streaming::new solver.rs:84-119) reads
+// the cell's own opposite slot instead.  The adjoint transposes the pull:
+// the same pattern with the velocities reversed (pull from x + c_q),
+// linearised at a recorded (rho, u).
 #pragma once
 #include <type_traits>
 
@@ -63,15 +62,23 @@ struct Cvt<__nv_bfloat16> {
     __device__ __forceinline__ static __nv_bfloat16 from(float v) { return __float2bfloat16_rn(v); }
 };
 
-// Stochastic rounding to the 16-bit formats: add uniform random bits below
-// the kept mantissa, then truncate.  A nearly steady state is re-rounded
+// Stochastic rounding to the 16-bit formats: FP16 through the hardware's
+// stochastic-rounding conversion; BF16 (FP32's exponent range, so no
+// subnormal halves to care about) by adding uniform random bits below the
+// kept mantissa and truncating.  A nearly steady state is re-rounded
 // every step; with round-to-nearest the same rounding errors repeat and the
 // mass drifts linearly in time, with stochastic rounding they average out.
 template <typename T>
 __device__ __forceinline__ T round_stochastic(float v, uint32_t r);
 template <>
 __device__ __forceinline__ __half round_stochastic<__half>(float v, uint32_t r) {
-    return __float2half_rz(__uint_as_float(__float_as_uint(v) + (r >> 19)));  // 13 dropped bits
+    // the hardware stochastic rounding (cvt.rs) drops the right number of
+    // bits for subnormal halves too, where adding a fixed 13 random bits
+    // below the normal mantissa would bias the result toward zero
+    // (r ^ r >> 16: the LCG's high bits reach both halves of the word)
+    uint32_t d;
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(0.f), "f"(v), "r"(r ^ (r >> 16)));
+    return __ushort_as_half((unsigned short)(d & 0xffffu));
 }
 template <>
 __device__ __forceinline__ __nv_bfloat16 round_stochastic<__nv_bfloat16>(float v, uint32_t r) {

@@ -1,4 +1,5 @@
-// lbm_launch.h -- host-side launchers of the sm_100a kernels (lbm_kernels.cu).
+// lbm_launch.h -- host-side launchers of the sm_100a kernels (lbm_forward.cu,
+// lbm_adjoint.cu, lbm_misc.cu).
 // Every launcher enqueues on the given stream and returns the launch status.
 #pragma once
 

@@ -48,8 +48,8 @@ __global__ void __launch_bounds__(NOALLOC_THREADS) k_state_stats(const float* __
     float minf = INFINITY, maxu2 = 0.f;
     int nf = 0;
     for (uint32_t x = blockIdx.x * NOALLOC_THREADS + threadIdx.x; x < n; x += gridDim.x * NOALLOC_THREADS) {
-        if (solid && solid[x]) continue;
         float rho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f, mn = INFINITY;
+        bool finite = true;
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const float v = f[q * n + x];
@@ -58,13 +58,17 @@ __global__ void __launch_bounds__(NOALLOC_THREADS) k_state_stats(const float* __
             if (L::cy(q)) jy += L::cy(q) * v;
             if (L::cz(q)) jz += L::cz(q) * v;
             mn = fminf(mn, v);
+            finite = finite && isfinite(v);
         }
+        // finiteness over every cell, solid ones included; the other
+        // statistics over fluid cells (solver.rs:714-726)
+        if (!finite) nf = 1;
+        if (solid && solid[x]) continue;
         const float s = 1.f + 0.5f * (alpha ? alpha[x] : 0.f);
         const float ux = (jx / rho + 0.5f * ax) / s, uy = (jy / rho + 0.5f * ay) / s, uz = (jz / rho + 0.5f * az) / s;
         mass += (double)rho;
         minf = fminf(minf, mn);
         maxu2 = fmaxf(maxu2, ux * ux + uy * uy + uz * uz);
-        if (!isfinite(rho)) nf = 1;
     }
     DiagAcc v;
     v.mh = mass;
@@ -119,7 +123,10 @@ std::mutex g_setup_mu;
 void* g_scratch_ptr[MAX_DEVICES] = {};
 
 // Device address of g_stats_scratch on the current device, looked up once per
-// device (the host-side name of the array is not a device address).
+// device (the host-side name of the array is not a device address).  The
+// cached address belongs to the device's primary context: after
+// cudaDeviceReset the module is loaded again and the array may move, so the
+// entry point must not be used on that device for the rest of the process.
 cudaError_t scratch_on_current_device(void** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);

@@ -365,6 +365,9 @@ struct lbm_handle {
     int cur = 0;   // which population array holds the current state
     int lcur = 0;  // which adjoint array holds the current adjoint state
     bool pending = false;
+    // a non-finite population was loaded into a solid cell (lbm_set_populations):
+    // solid cells are never stepped, so every later state carries it too
+    bool solid_nonfinite = false;
     int64_t t = 0;
     std::string err;
 
@@ -877,6 +880,7 @@ void init_state(lbm_handle& h) {
     h.pending = false;
     h.t = 0;
     h.state_valid = true;
+    h.solid_nonfinite = false;
 }
 
 void require_design(const lbm_handle& h) {
@@ -895,7 +899,9 @@ double mass_drift_limit(int storage) {
 // Admission from the per-state records (solver.rs:708-793).
 lbm_status admit(lbm_handle& h, const std::vector<StepDiag>& d, lbm_diag_t* out, double ms) {
     const size_t T = d.size();
-    bool nonfinite = false;
+    // finiteness covers every cell (solid ones through the load-time check),
+    // the minimum only fluid cells (solver.rs:714-726)
+    bool nonfinite = h.solid_nonfinite;
     double minimum = INFINITY, maxu2 = 0;
     for (auto& s : d) {
         nonfinite = nonfinite || s.nonfinite;
@@ -1821,8 +1827,12 @@ lbm_status lbm_set_populations(lbm_handle* h, const double* f, size_t n) {
         const int Q = h->Q;
         check_n(*h, n, (size_t)(N * Q), "populations");
         std::vector<float> g((size_t)N * Q);
-        for (int64_t x = 0; x < N; ++x)
+        bool solid_nonfinite = false;
+        for (int64_t x = 0; x < N; ++x) {
             for (int q = 0; q < Q; ++q) g[(size_t)q * N + x] = (float)(f[x * Q + q] - h->L.w[q]);
+            if (h->cls[x] == 0)  // solid
+                for (int q = 0; q < Q; ++q) solid_nonfinite = solid_nonfinite || !std::isfinite(f[x * Q + q]);
+        }
         ensure_scratch(*h);
         CK(cudaMemcpyAsync(h->scratch.p, g.data(), g.size() * 4, cudaMemcpyHostToDevice, h->stream));
         const int grid = grid_for(*h);
@@ -1835,6 +1845,7 @@ lbm_status lbm_set_populations(lbm_handle* h, const double* f, size_t n) {
         h->t = 0;
         h->state_valid = true;
         h->forward_done = false;
+        h->solid_nonfinite = solid_nonfinite;
         return LBM_OK;
     });
 }

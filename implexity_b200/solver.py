@@ -73,6 +73,7 @@ class Diagnostics:
     steps: int
     admitted: bool
     device_ms: float
+    nonfinite: bool = False
 
     @classmethod
     def of(cls, d: _abi.Diag) -> "Diagnostics":
@@ -85,6 +86,7 @@ class Diagnostics:
             int(d.steps),
             bool(d.admitted),
             d.device_ms,
+            bool(d.nonfinite),
         )
 
 

@@ -379,13 +379,18 @@ LBM_API lbm_status lbm_design_vjp(lbm_handle* h, const double* phi_bar, double* 
  * every step (LbmProblem::admit quantities, solver.rs:714-755).
  *
  *   populations  device, FP32, plane-major f[q*cells + cell] (unshifted f),
- *                velocity order of the lattice as in lbm_get_populations
+ *                velocity order of the lattice as in lbm_get_populations.
+ *                A state held in 16-bit or shifted form (such as this
+ *                library's (f - w)/w storage) must be expanded to unshifted
+ *                FP32 by the caller first: there is no scratch for a
+ *                conversion here.
  *   solid        device uint8 per cell, NULL = all fluid (solid cells skipped)
  *   alpha        device FP32 Brinkman resistance per cell, NULL = 0
  *   acceleration_lattice  host, 3 doubles, NULL = 0
- *   out4         device, 4 doubles: fluid mass sum(rho), minimum population,
- *                maximum |u| (implicit half-step Brinkman velocity), and 1.0
- *                if any population is non-finite (else 0.0)
+ *   out4         device, 4 doubles: fluid mass sum(rho), minimum population
+ *                over fluid cells, maximum |u| over fluid cells (implicit
+ *                half-step Brinkman velocity), and 1.0 if any population of
+ *                any cell, solid ones included, is non-finite (else 0.0)
  *   stream       cudaStream_t, NULL = the legacy default stream
  *
  * It allocates nothing: its scratch (per-block partials and a ticket counter)
@@ -393,7 +398,9 @@ LBM_API lbm_status lbm_design_vjp(lbm_handle* h, const double* phi_bar, double* 
  * holds until the process exits.  Limit: q * cells < 2^31 (larger states are
  * rejected with LBM_E_CONTRACT); any such state is covered with at most 1024
  * blocks.  The first call on a device looks up the array's device address on
- * that device, so make that first call before any stream capture.  The call is
+ * that device, so make that first call before any stream capture.  The
+ * address is kept for the process: after cudaDeviceReset on a device the
+ * entry point must not be used on that device again.  The call is
  * asynchronous on `stream`: out4 is written when the stream reaches the
  * kernel.  All calls share the one array, so calls that overlap on the GPU
  * (other streams, other host threads, same device) race and must be ordered

@@ -8,6 +8,9 @@ import pytest
 ROOT = Path(__file__).resolve().parent.parent
 if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
+GOLDEN = ROOT / "tests" / "golden"
+if str(GOLDEN) not in sys.path:
+    sys.path.insert(0, str(GOLDEN))
 
 
 def pytest_configure(config):

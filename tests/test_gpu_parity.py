@@ -6,7 +6,8 @@ Tolerances (FP32 arithmetic and storage unless stated):
                                      against 1e-5 of the axial one)
   one transposed step                relative L2 <= 1e-5
   design gradient                    relative L2 <= 1e-4
-  FP16 storage                       velocity 2e-3, gradient relative L2 <= 1e-3
+  FP16 / BF16 storage (vs FP64)      velocity 2e-3 / 2e-2, gradient relative
+                                     L2 <= 1e-3 / 1e-2
 """
 import numpy as np
 import pytest
@@ -191,22 +192,31 @@ def test_steady_gradient_matches_oracle(gpu_lib):
     assert rel_l2(g, g_ref) < 1e-4, rel_l2(g, g_ref)
 
 
-def test_fp16_storage_close_to_fp32(gpu_lib):
-    prob32, norm, raw = make("trt", "D3Q19", steps=600)
-    prob16, _, _ = make("trt", "D3Q19", steps=600, storage="float16")
+def _sixteen_bit_against_oracle(storage, u_tol, g_tol):
+    """16-bit storage of (f - w)/w against the FP64 oracle: velocity of the
+    final state (max norm) and the steady gradient (relative L2)."""
+    prob, norm, raw = make("trt", "D3Q19", steps=600, storage=storage)
     w = workloads.objective_weights()
-    with LbmSolver(prob32) as s32, LbmSolver(prob16) as s16:
-        for s in (s32, s16):
-            s.set_design(raw)
-            s.forward()
-        f32, f16 = s32.populations(), s16.populations()
-        _, alpha = s32.design()
-        _, u32 = macroscopic(f32, 19, alpha.ravel(), s32.acceleration_lattice)
-        _, u16 = macroscopic(f16, 19, alpha.ravel(), s16.acceleration_lattice)
-        assert rel_max(u16, u32) < 2e-3
-        g32, _ = s32.gradient(w, mode="steady", tolerance=1e-8)
-        g16, _ = s16.gradient(w, mode="steady", tolerance=1e-8, lambda_storage="float16")
-        assert rel_l2(g16, g32) < 1e-3, rel_l2(g16, g32)
+    o = Oracle(norm)
+    _, alpha = o.design(raw)
+    f_ref, _ = o.history(alpha, norm.step_count)
+    g_ref, _, _, st = o.gradient(raw, w, mode="steady", tol=1e-12)
+    assert st == 0
+    with LbmSolver(prob) as s:
+        s.set_design(raw)
+        s.forward()
+        f = s.populations()
+        g, rep = s.gradient(w, mode="steady", tolerance=1e-8, lambda_storage=storage)
+    assert rep.converged
+    _, u = macroscopic(f, 19, alpha, o.acceleration_lattice)
+    _, u_ref = macroscopic(f_ref, 19, alpha, o.acceleration_lattice)
+    assert rel_max(u, u_ref) < u_tol, rel_max(u, u_ref)
+    assert rel_l2(g, g_ref) < g_tol, rel_l2(g, g_ref)
+
+
+def test_fp16_storage_against_fp64_oracle(gpu_lib):
+    """FP16 storage (10 mantissa bits): velocity 2e-3, gradient 1e-3."""
+    _sixteen_bit_against_oracle("float16", 2e-3, 1e-3)
 
 
 def solid_channel(lattice, storage="float32", steps=60, periodic=(False, False, False)):
@@ -370,21 +380,31 @@ def test_mrt_with_even_rate_matches_oracle(gpu_lib, lattice):
     assert rel_l2(g, g_ref) < 1e-4, rel_l2(g, g_ref)
 
 
-def test_bf16_storage_close_to_fp32(gpu_lib):
-    """BF16 storage of (f - w)/w (8 mantissa bits): velocity and steady
-    gradient stay within the format's resolution of the FP32 run."""
-    prob32, norm, raw = make("trt", "D3Q19", steps=600)
-    prob16, _, _ = make("trt", "D3Q19", steps=600, storage="bfloat16")
-    w = workloads.objective_weights()
-    with LbmSolver(prob32) as s32, LbmSolver(prob16) as s16:
-        for s in (s32, s16):
-            s.set_design(raw)
-            s.forward()
-        f32, f16 = s32.populations(), s16.populations()
-        _, alpha = s32.design()
-        _, u32 = macroscopic(f32, 19, alpha.ravel(), s32.acceleration_lattice)
-        _, u16 = macroscopic(f16, 19, alpha.ravel(), s16.acceleration_lattice)
-        assert rel_max(u16, u32) < 2e-2, rel_max(u16, u32)
-        g32, _ = s32.gradient(w, mode="steady", tolerance=1e-8)
-        g16, _ = s16.gradient(w, mode="steady", tolerance=1e-8, lambda_storage="bfloat16")
-        assert rel_l2(g16, g32) < 1e-2, rel_l2(g16, g32)
+def test_bf16_storage_against_fp64_oracle(gpu_lib):
+    """BF16 storage (7 mantissa bits): velocity 2e-2, gradient 1e-2."""
+    _sixteen_bit_against_oracle("bfloat16", 2e-2, 1e-2)
+
+
+def test_nonfinite_population_in_a_solid_cell_is_refused(gpu_lib):
+    """admit (solver.rs:714-719) checks finiteness over every cell, solid ones
+    included, and the minimum over fluid cells: a NaN loaded into a solid cell
+    refuses the trajectory; a clean reload is admitted again."""
+    from implexity_b200 import ContractError
+
+    shape = (12, 9, 8)
+    solid = np.zeros(shape, bool)
+    solid[5:7, 3:5, 3:5] = True
+    prob = workloads.channel_problem(shape=shape, steps=20, collision="trt", solid=solid)
+    raw = workloads.uniform_design(shape, 2)
+    with LbmSolver(prob) as s:
+        s.set_design(raw)
+        s.forward()
+        f = s.populations()
+        bad = f.copy()
+        bad[int(np.flatnonzero(solid.ravel())[0]), 4] = np.nan
+        s.set_populations(bad)
+        with pytest.raises(ContractError, match="nonpositive or nonfinite"):
+            s.advance(3)
+        assert s.last_diag.nonfinite
+        s.set_populations(f)
+        assert s.advance(3).admitted

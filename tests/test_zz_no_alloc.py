@@ -23,13 +23,24 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr())
 
 
-def test_noalloc_stats_match_forward_record(gpu_lib):
+CASES = [
+    # a small channel with a solid block: 10 blocks, one cell per thread
+    ("D3Q19", (20, 12, 10), 80),
+    # 294 912 cells: the grid is capped at the 1024 blocks the static array
+    # holds partials for, each thread covers several cells, and the last block
+    # merges a full partials array
+    ("D3Q19", (72, 64, 64), 10),
+    ("D3Q27", (20, 12, 10), 80),
+]
+
+
+@pytest.mark.parametrize("lattice,shape,steps", CASES)
+def test_noalloc_stats_match_forward_record(gpu_lib, lattice, shape, steps):
     import torch
 
-    shape = (20, 12, 10)
     solid = np.zeros(shape, bool)
     solid[9:11, 5:7, 4:6] = True
-    prob = workloads.channel_problem(shape=shape, steps=80, collision="trt", solid=solid)
+    prob = workloads.channel_problem(shape=shape, steps=steps, collision="trt", lattice=lattice, solid=solid)
     norm = normalize(prob)
     raw = workloads.uniform_design(shape, 5)
     with LbmSolver(norm) as s:
@@ -61,6 +72,21 @@ def test_noalloc_stats_match_forward_record(gpu_lib):
     assert abs(mass - traj["mass"][-1]) <= 1e-5 * traj["mass"][-1]
     assert abs(min_pop - traj["min_population"][-1]) <= 1e-5 * abs(traj["min_population"][-1])
     assert abs(max_speed - traj["max_speed"][-1]) <= 1e-5 * traj["max_speed"][-1]
+    # the same sums in FP64 on the host
+    fluid = ~solid.ravel()
+    assert abs(mass - f[fluid].sum()) <= 1e-6 * mass
+
+    # a non-finite population in a solid cell is reported too, and the next
+    # call on a clean state clears the flag again
+    x = int(np.flatnonzero(solid.ravel())[0])
+    f_bad = f_dev.clone()
+    f_bad[3, x] = float("nan")
+    for state, flag in ((f_bad, 1.0), (f_dev, 0.0)):
+        st = gpu_lib.lbm_state_stats_noalloc(q, cells, _ptr(state), _ptr(solid_dev), _ptr(alpha_dev), acc, _ptr(out),
+                                             stream)
+        assert st == _abi.LBM_OK, gpu_lib.lbm_last_error(None).decode()
+        torch.cuda.synchronize(dev)
+        assert out.cpu().numpy()[3] == flag
 
 
 def test_noalloc_rejects_oversized_state(gpu_lib):
