@@ -9,7 +9,7 @@ import ctypes as C
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "liblbm_b200.so"
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 # status codes
 LBM_OK, LBM_E_CONTRACT, LBM_E_CONVERGENCE, LBM_E_CUDA, LBM_E_STATE = 0, 1, 2, 3, 4
@@ -127,6 +127,7 @@ class AdjointOpts(C.Structure):
         ("objective", C.c_int32),
         ("checkpointing", C.c_int32),
         ("snapshots", C.c_int64),
+        ("steady_solver", C.c_int32),
     ]
 
 

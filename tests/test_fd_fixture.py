@@ -38,6 +38,7 @@ def test_oracle_fd_at_step_1e4_matches_gpu_adjoint(gpu_lib):
         s.forward()
         J = float(np.dot(w, s.responses()))
         g_h, _ = s.gradient(w, mode="horizon", checkpoint_every=100)
+        s.forward()  # the horizon adjoint's recomputation leaves the state elsewhere
         g_s, rep = s.gradient(w, mode="steady", tolerance=1e-10)
     assert rep.converged
     assert abs(J - float(fx["objective"])) <= 1e-6 * abs(float(fx["objective"]))
