@@ -98,6 +98,7 @@ class Problem(C.Structure):
         ("fixed_design", C.POINTER(C.c_double)),
         ("ports", C.POINTER(Port)),
         ("time_average", C.c_int32),
+        ("collision_fp64", C.c_int32),
     ]
 
 
@@ -127,7 +128,6 @@ class AdjointOpts(C.Structure):
         ("objective", C.c_int32),
         ("checkpointing", C.c_int32),
         ("snapshots", C.c_int64),
-        ("steady_solver", C.c_int32),
     ]
 
 

@@ -23,7 +23,7 @@ MMA_SOURCE = CSRC / "mma_cpu.cpp"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
-SOURCES = ["lbm_forward.cu", "lbm_adjoint.cu", "lbm_misc.cu", "lbm_krylov.cu", "lbm_noalloc.cu", "lbm_runtime.cpp"]
+SOURCES = ["lbm_forward.cu", "lbm_adjoint.cu", "lbm_misc.cu", "lbm_noalloc.cu", "lbm_runtime.cpp"]
 
 
 def nvcc() -> str:

@@ -25,10 +25,7 @@ struct AdjStage {
 
 // STG = 1: the stage-objective variant, which reads the second moments of
 // the recorded state as well and adds the state's response VJP.
-// KRY = 1: the operator of the Krylov steady adjoint (FP32 storage): the
-// stored output is in_own - (transposed step of in), and the dot products
-// the solver needs are summed on the way out.
-template <int Q, int COLL, typename T, int AL, int STG, int KRY>
+template <int Q, int COLL, typename T, int AL, int STG>
 __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
     constexpr int NREC = STG ? 10 : 4;
     using S = AdjStage<Q, T, NREC>;
@@ -43,7 +40,6 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
     const uint32_t ntiles = (n + TILE - 1) / TILE;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double nsum = 0.0;
-    double kd[3] = {0.0, 0.0, 0.0};  // KRY: <rhat, out>, <in_own, out>, <out, out>
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int s = 0; s < STAGES; ++s) {
@@ -135,18 +131,6 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
                 }
                 a.abar[x] = fmaf(ab, a.abar_factor, ab_prev);
                 if (a.port_transpose && (m & MASK_PORT)) port_transpose<Q>(a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], v);
-                if constexpr (KRY) {
-                    // (I - L) in: the input's own slots minus the transposed step
-#pragma unroll
-                    for (int q = 0; q < Q; ++q) {
-                        const float own = Cvt<T>::to(B[q * n + x]);
-                        const float o = own - v[q];
-                        v[q] = o;
-                        kd[1] += (double)own * (double)o;
-                        kd[2] += (double)o * (double)o;
-                        if (a.kry_rhat) kd[0] += (double)a.kry_rhat[q * n + x] * (double)o;
-                    }
-                }
                 store_own_lam<Q, T>(D, n, x, v, k_out);
                 if (a.norm2) {
 #pragma unroll
@@ -164,13 +148,7 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
             }
         }
     }
-    if constexpr (KRY) {
-        Sums<3> sm;
-        sm.init();
-#pragma unroll
-        for (int k = 0; k < 3; ++k) sm.h[k] = kd[k];
-        finish_sums<3>(sm, a.kry_dots, a.red);
-    } else if (a.norm2) {
+    if (a.norm2) {
         Sums<1> sm;
         sm.init();
         sm.h[0] = nsum;
@@ -178,17 +156,17 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
     }
 }
 
-template <int Q, int COLL, typename T, int AL, int STG, int KRY = 0>
+template <int Q, int COLL, typename T, int AL, int STG>
 cudaError_t run_adjoint_al(const AdjArgs& a, cudaStream_t s) {
     constexpr size_t smem = pipe_bytes<AdjStage<Q, T, STG ? 10 : 4>, ring_depth<AdjStage<Q, T, STG ? 10 : 4>, T>()>();
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = set_smem(k_adjoint<Q, COLL, T, AL, STG, KRY>, smem);
+        cudaError_t e = set_smem(k_adjoint<Q, COLL, T, AL, STG>, smem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    const int grid = persistent_grid((const void*)k_adjoint<Q, COLL, T, AL, STG, KRY>, a.G.n, smem, TPB, TILE);
-    k_adjoint<Q, COLL, T, AL, STG, KRY><<<grid, TPB, smem, s>>>(a);
+    const int grid = persistent_grid((const void*)k_adjoint<Q, COLL, T, AL, STG>, a.G.n, smem, TPB, TILE);
+    k_adjoint<Q, COLL, T, AL, STG><<<grid, TPB, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -204,15 +182,6 @@ bool adj_table_is_aligned(const int32_t* rund) {
 template <int Q, int COLL, typename T>
 cudaError_t run_adjoint(const AdjArgs& a, cudaStream_t s) {
     const bool al = adj_table_is_aligned<Q, T>(a.rund);
-    if (a.kry) {
-        // the Krylov operator: FP32 vectors, final-state record only
-        if constexpr (std::is_same<T, float>::value) {
-            if (a.rec_planes != 4 || a.stage || !a.kry_dots) return cudaErrorInvalidValue;
-            return al ? run_adjoint_al<Q, COLL, T, 1, 0, 1>(a, s) : run_adjoint_al<Q, COLL, T, 0, 0, 1>(a, s);
-        } else {
-            return cudaErrorInvalidValue;
-        }
-    }
     if (a.rec_planes == 10)
         return al ? run_adjoint_al<Q, COLL, T, 1, 1>(a, s) : run_adjoint_al<Q, COLL, T, 0, 1>(a, s);
     return al ? run_adjoint_al<Q, COLL, T, 1, 0>(a, s) : run_adjoint_al<Q, COLL, T, 0, 0>(a, s);

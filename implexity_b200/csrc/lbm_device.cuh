@@ -307,6 +307,16 @@ __device__ __forceinline__ Macro macroscopic(const float (&g)[Q], float alpha, c
 }
 
 template <int Q>
+__device__ __forceinline__ double dotc_d(int q, const double (&v)[3]) {
+    using L = Lat<Q>;
+    double s = 0.0;
+    if (L::cx(q)) s += L::cx(q) * v[0];
+    if (L::cy(q)) s += L::cy(q) * v[1];
+    if (L::cz(q)) s += L::cz(q) * v[2];
+    return s;
+}
+
+template <int Q>
 __device__ __forceinline__ float dotc(int q, const float (&v)[3]) {
     using L = Lat<Q>;
     float s = 0.f;
@@ -481,6 +491,124 @@ __device__ __forceinline__ Macro collide_fused(float (&v)[Q], float alpha, const
         }
     }
     v[0] = SC ? rem * (float)(1.0 / L::wd(0)) : rem;
+    return M;
+}
+
+// The same collision in FP64 arithmetic for FP32 storage (g = f - w form):
+// the populations are widened once, collided with the exact weights, and
+// rounded once on the way out.  FP32 arithmetic rounds the equilibrium
+// momentum (rho u, the weights) to ~1e-7 relative, and in a nearly uniform
+// flow those roundings repeat coherently from cell to cell and step to step:
+// the steady state then carries a bias of ~1e-7 in density (the pressure drop
+// ~1e-6 relative on the 64^3 channel), where the stored state's own rounding
+// alone leaves ~1e-9.  Selected per problem (collision_fp64); the rates and
+// MRT basis vectors are the FP32 ones of Physics.
+template <int Q, int COLL>
+__device__ __forceinline__ Macro collide_fused_dp(float (&vf)[Q], float alpha_f, const Physics& P, bool post) {
+    using L = Lat<Q>;
+    constexpr int NP = L::NPAIR;
+    double v[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) v[q] = vf[q];
+    double S[NP], D[NP];
+    double rp = v[0], j[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        const int i = k + 1, o = opp<Q>(i);
+        S[k] = v[i] + v[o];
+        D[k] = v[i] - v[o];
+        rp += S[k];
+        if (L::cx(i)) j[0] += L::cx(i) * D[k];
+        if (L::cy(i)) j[1] += L::cy(i) * D[k];
+        if (L::cz(i)) j[2] += L::cz(i) * D[k];
+    }
+    const double alpha = alpha_f, rho = 1.0 + rp, s = 1.0 + 0.5 * alpha;
+    double u[3], F[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        u[d] = (j[d] / rho + 0.5 * (double)P.a[d]) / s;
+        F[d] = rho * ((double)P.a[d] - alpha * u[d]);
+    }
+    Macro M;
+    M.rp = (float)rp;
+    M.rho = (float)rho;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        M.u[d] = (float)u[d];
+        M.F[d] = (float)F[d];
+    }
+    if (!post) return M;
+    const double om = P.omega, omm = P.om;
+    const double kp = 1.0 - 0.5 * om, km = 1.0 - 0.5 * omm;
+    const double hp = 0.5 * (1.0 - om), hm = 0.5 * (1.0 - omm);
+    const double usq15 = 1.5 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const double uf3 = 3.0 * (u[0] * F[0] + u[1] * F[1] + u[2] * F[2]);
+    // y = f - eq + src/2 of the rest population (MRT projections)
+    const double y0 = v[0] - L::wd(0) * (rp - rho * usq15) - 0.5 * L::wd(0) * uf3;
+    double dproj[MAX_PROJ];
+#pragma unroll
+    for (int p = 0; p < MAX_PROJ; ++p) dproj[p] = (COLL == CK_MRT && p < P.n_proj) ? (double)P.proj_right[p][0] * y0 : 0.0;
+    double Eb = -y0;  // MRT_BULK: sum_i w_i b_i y_i with b = |c|^2 - 1
+    double rem = rp;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        const int i = k + 1, o = opp<Q>(i);
+        const double w = L::wd(i);
+        const double cu = dotc_d<Q>(i, u), cf = dotc_d<Q>(i, F);
+        const double geqp = w * (rho * (4.5 * cu * cu - usq15) + rp);  // symmetric part of eq (g form)
+        const double eqm = 3.0 * w * rho * cu;                          // antisymmetric part
+        const double spv = w * (9.0 * cu * cf - uf3);                    // symmetric part of the source
+        const double smv = 3.0 * w * cf;                                 // antisymmetric part
+        if constexpr (COLL == CK_MRT_BULK) {
+            const int c2 = L::cx(i) * L::cx(i) + L::cy(i) * L::cy(i) + L::cz(i) * L::cz(i);
+            if (c2 != 1) Eb += 2.0 * (c2 - 1) * (0.5 * S[k] - geqp + 0.5 * spv);
+        }
+        if constexpr (COLL == CK_MRT) {
+            const double yp = 0.5 * S[k] - geqp + 0.5 * spv;
+#pragma unroll
+            for (int p = 0; p < MAX_PROJ; ++p)
+                if (p < P.n_proj) dproj[p] += 2.0 * (double)P.proj_right[p][i] * yp;
+        }
+        const double Pp = hp * S[k] + kp * spv + om * geqp;
+        const double Dm = hm * D[k] + km * smv + omm * eqm;
+        v[i] = Pp + Dm;
+        v[o] = Pp - Dm;
+        rem -= 2.0 * Pp;
+    }
+    if constexpr (COLL == CK_MRT_BULK) {
+        // rank-one bulk correction, |b|^2_W = 2/3; the rest population keeps the mass
+        const double cb = (double)P.proj_rate[0] * Eb * 1.5;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            const int i = k + 1, o = opp<Q>(i);
+            const int c2 = L::cx(i) * L::cx(i) + L::cy(i) * L::cy(i) + L::cz(i) * L::cz(i);
+            if (c2 != 1) {
+                const double dv = cb * (c2 - 1) * L::wd(i);
+                v[i] -= dv;
+                v[o] -= dv;
+                rem += 2.0 * dv;
+            }
+        }
+    }
+    if constexpr (COLL == CK_MRT) {
+#pragma unroll
+        for (int p = 0; p < MAX_PROJ; ++p) {
+            if (p < P.n_proj) {
+                const double c = (double)P.proj_rate[p] * dproj[p];
+#pragma unroll
+                for (int k = 0; k < NP; ++k) {
+                    const int i = k + 1, o = opp<Q>(i);
+                    const double dv = c * (double)P.proj_left[p][i];
+                    v[i] -= dv;
+                    v[o] -= dv;
+                    rem += 2.0 * dv;
+                }
+            }
+        }
+    }
+    v[0] = rem;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) vf[q] = (float)v[q];
     return M;
 }
 

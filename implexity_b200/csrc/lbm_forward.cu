@@ -24,7 +24,8 @@ struct FwdStage {
 
 // RSP = 1: the step also sums the responses of the state it reads (the
 // stage objective's per-state values; vector_cell, solver.rs:835-895).
-template <int Q, int COLL, typename T, int AL, int RSP>
+// DP = 1: FP64 collision arithmetic (FP32 storage only; collide_fused_dp).
+template <int Q, int COLL, typename T, int AL, int RSP, int DP>
 __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
     using L = Lat<Q>;
     using S = FwdStage<Q, T>;
@@ -156,7 +157,9 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
                         for (int e = 0; e < 6; ++e) a.record[(size_t)(4 + e) * n + x] = S[e];
                     }
                 }
-                const Macro M = collide_fused<Q, COLL, SC>(v, alpha, a.P, a.collide);
+                Macro M;
+                if constexpr (DP) M = collide_fused_dp<Q, COLL>(v, alpha, a.P, a.collide);
+                else M = collide_fused<Q, COLL, SC>(v, alpha, a.P, a.collide);
                 if constexpr (RSP) {
                     float r6[6];
                     response_cell<Q>(M.rp, M.u, S, alpha, a.sp, a.P, r6);
@@ -220,23 +223,30 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
     }
 }
 
-template <int Q, int COLL, typename T, int AL, int RSP>
+template <int Q, int COLL, typename T, int AL, int RSP, int DP>
 cudaError_t run_forward_rs(const FwdArgs& a, cudaStream_t s) {
     constexpr size_t smem = pipe_bytes<FwdStage<Q, T>, ring_depth<FwdStage<Q, T>, T>()>();
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = set_smem(k_forward<Q, COLL, T, AL, RSP>, smem);
+        cudaError_t e = set_smem(k_forward<Q, COLL, T, AL, RSP, DP>, smem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    const int grid = persistent_grid((const void*)k_forward<Q, COLL, T, AL, RSP>, a.G.n, smem, TPB, TILE);
-    k_forward<Q, COLL, T, AL, RSP><<<grid, TPB, smem, s>>>(a);
+    const int grid = persistent_grid((const void*)k_forward<Q, COLL, T, AL, RSP, DP>, a.G.n, smem, TPB, TILE);
+    k_forward<Q, COLL, T, AL, RSP, DP><<<grid, TPB, smem, s>>>(a);
     return cudaGetLastError();
 }
 
 template <int Q, int COLL, typename T, int AL>
 cudaError_t run_forward_al(const FwdArgs& a, cudaStream_t s) {
-    return a.stage ? run_forward_rs<Q, COLL, T, AL, 1>(a, s) : run_forward_rs<Q, COLL, T, AL, 0>(a, s);
+    if (a.dp_collision) {
+        // FP64 collision arithmetic exists for FP32 storage only
+        if constexpr (std::is_same<T, float>::value)
+            return a.stage ? run_forward_rs<Q, COLL, T, AL, 1, 1>(a, s) : run_forward_rs<Q, COLL, T, AL, 0, 1>(a, s);
+        else
+            return cudaErrorInvalidValue;
+    }
+    return a.stage ? run_forward_rs<Q, COLL, T, AL, 1, 0>(a, s) : run_forward_rs<Q, COLL, T, AL, 0, 0>(a, s);
 }
 
 // The run offsets are compile-time constants when every run table entry

@@ -1,5 +1,5 @@
 // lbm_launch.h -- host-side launchers of the sm_100a kernels (lbm_forward.cu,
-// lbm_adjoint.cu, lbm_misc.cu, lbm_krylov.cu).
+// lbm_adjoint.cu, lbm_misc.cu).
 // Every launcher enqueues on the given stream and returns the launch status.
 #pragma once
 
@@ -50,6 +50,7 @@ struct FwdArgs {
     // inside it
     int64_t run0[27];
     int32_t rund[27];
+    int32_t dp_collision;    // FP64 collision arithmetic (FP32 storage)
 };
 
 struct AdjArgs {
@@ -77,13 +78,6 @@ struct AdjArgs {
     int32_t rund[27];
     int64_t rec0[10];        // staged record runs
     int32_t recd[10];
-    // BiCGStab operator (FP32 adjoint storage, unit scales): the step stores
-    // out = in_own - Ports^T C^T S^T in, i.e. (I - L) applied to the input
-    // vector, and sums <kry_rhat, out>, <in_own, out>, <out, out> into
-    // kry_dots (three compensated pairs; kry_rhat may be null)
-    int32_t kry;
-    const float* kry_rhat;
-    double* kry_dots;
 };
 
 struct ObjArgs {
@@ -135,32 +129,6 @@ struct DesignArgs {
     float* scale;
     float* grad;
 };
-
-// BiCGStab steady adjoint (lbm_krylov.cu).  Scalar block (doubles): the two
-// operator launches of an iteration write their dot products (three
-// compensated pairs each) at SC_K1 and SC_K3, the residual update its two at
-// SC_KR; the scalars are written by one thread of the kernel that forms them
-// and read only by later launches.
-enum : int {
-    SC_K1 = 0,        // <rhat, v>, <p, v>, <v, v>      (v = (I - L) p)
-    SC_K3 = 6,        // <rhat, t>, <s, t>, <t, t>      (t = (I - L) s)
-    SC_KR = 12,       // <rhat, r>, <r, r>
-    SC_RHO_PREV = 16, // rho of the iteration (<rhat, r> before the update)
-    SC_ALPHA = 17,
-    SC_OMEGA = 18,
-    SC_SIZE = 32
-};
-enum KryOp { KRY_INIT = 0, KRY_S = 1, KRY_R = 2, KRY_P = 3 };
-struct KryVectors {
-    int64_t n;
-    const uint32_t* mask;
-    float *r, *rhat, *p, *v, *s, *t;  // FP32, Q planes of n cells each
-    float* abar;                      // accumulated alpha cotangent
-    const float *abar_p, *abar_s;     // per-cell alpha cotangents of the two operator launches
-    double* sc;                       // scalar block (SC_SIZE doubles)
-    Reduce red;
-};
-cudaError_t launch_krylov(int Q, int op, const KryVectors& kv, int grid, cudaStream_t s);
 
 // Fills run0/rund for a tile-staged kernel: direction q's run starts at the
 // first used element q*n + x0 + dir*lin(q) (dir -1: forward pull, +1:

@@ -321,6 +321,7 @@ struct Checkpoint {
 struct lbm_handle {
     // --- normalised problem
     int Q = 19, coll = LBM_BGK, storage = LBM_STORE_F32;
+    bool collision_fp64 = false;  // FP64 collision arithmetic on FP32 storage
     Geometry G{};
     Physics P{};
     HostLat L{};
@@ -340,7 +341,6 @@ struct lbm_handle {
     int64_t device_bytes = 0;
     DevBuf pop, mask, alpha, phi, raw, den, slope, cls_d, fixed_d, offsets_d, ports_d, partial, counter, diag;
     DevBuf lam, record, abar, abar_final, phibar, scale, grad, norm2, sums, scratch, errflag;
-    DevBuf kry, kry_abar, kry_sc;  // BiCGStab steady adjoint: six FP32 vectors, two alpha cotangents, scalars
     int lam_storage = LBM_STORE_F32;
     // --- ports: normalised specs with their signals; pulsatile ports keep one
     // set of maps per state index on the device (ensure_port_maps)
@@ -517,9 +517,12 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
 
     require((uint64_t)n * (uint64_t)p.lattice < (1ull << 32),
             "grid too large for one device: Q * cells must stay below 2^32 populations");
+    require(!p.collision_fp64 || p.storage == LBM_STORE_F32,
+            "collision_arithmetic float64 needs population_storage float32");
     h.Q = p.lattice;
     h.coll = p.collision;
     h.storage = p.storage;
+    h.collision_fp64 = p.collision_fp64 != 0;
     h.L = host_lat(h.Q);
     h.G.n = n;
     h.G.nx = p.shape[0];
@@ -833,6 +836,7 @@ FwdArgs fwd_args(lbm_handle& h) {
     a.sp.dens = (float)h.density;
     a.sp.dt_s = (float)h.dt;
     a.sp.tau = (float)h.tau;
+    a.dp_collision = h.collision_fp64 ? 1 : 0;
     return a;
 }
 
@@ -1188,8 +1192,7 @@ SeedParams stage_seed(const lbm_handle& h, const double* w, double scale) {
     return sp;
 }
 
-double seed(lbm_handle& h, const double* w, AdjState& st, float* record, double stage_scale = 1.0,
-            void* lam_out = nullptr) {
+double seed(lbm_handle& h, const double* w, AdjState& st, float* record, double stage_scale = 1.0) {
     int64_t* ctr = &h.device_bytes;
     const int64_t n = h.n();
     h.abar_final.alloc((size_t)n * 4, ctr);
@@ -1197,7 +1200,7 @@ double seed(lbm_handle& h, const double* w, AdjState& st, float* record, double 
     h.norm2.alloc(2 * sizeof(double), ctr);
     ObjArgs a = obj_args(h);
     response_weights(h, w, stage_scale, a.w);
-    a.lam = lam_out ? lam_out : h.lamA();
+    a.lam = h.lamA();
     a.abar_final = h.abar_final.as<float>();
     a.phibar = h.phibar.as<float>();
     a.record = record;
@@ -1313,140 +1316,6 @@ lbm_status gradient_steady(lbm_handle& h, const double* w, const lbm_adjoint_opt
     if (!converged)
         throw ConvergenceError("steady adjoint did not reach the residual tolerance within max_iterations (residual=" +
                                repr_float(resid) + ")");
-    return LBM_OK;
-}
-
-// The steady adjoint by BiCGStab on (I - L) x = s (the seed), L the transposed
-// step at the final state.  Each iteration applies I - L twice (the fused
-// adjoint kernel, which also sums the dot products it sees) and updates the
-// vectors on the device (lbm_krylov.cu); the alpha cotangent B^T x
-// accumulates from the operator launches' per-cell outputs, so x is never
-// formed.  The residual |r| / |s| is read every few iterations.
-lbm_status gradient_steady_bicgstab(lbm_handle& h, const double* w, const lbm_adjoint_opts_t& o, double* grad,
-                                    lbm_adjoint_report_t* rep) {
-    if (!h.forward_done) throw StateError("lbm_forward must succeed before lbm_gradient");
-    if (o.lambda_storage != LBM_STORE_F32)
-        throw ContractError("the BiCGStab steady adjoint keeps its vectors in float32: lambda_storage must be float32");
-    int64_t* ctr = &h.device_bytes;
-    const int64_t n = h.n();
-    const size_t vb = h.array_bytes(LBM_STORE_F32);
-    const bool fresh = !h.kry.p;
-    h.kry.alloc(6 * vb, ctr);
-    if (fresh) CK(cudaMemsetAsync(h.kry.p, 0, 6 * vb, h.stream));  // solid slots stay zero in every vector
-    h.kry_abar.alloc(2 * ((size_t)n + CELL_PAD) * sizeof(float), ctr);
-    h.kry_sc.alloc(SC_SIZE * sizeof(double), ctr);
-    h.abar.alloc((size_t)n * 4, ctr);
-    h.norm2.alloc(2 * sizeof(double), ctr);
-    h.record.alloc(((size_t)n * 4 + CELL_PAD) * sizeof(float), ctr);
-    auto vec = [&](int k) {
-        return reinterpret_cast<float*>(static_cast<char*>(h.kry.p) + (size_t)k * vb) + pop_pad(h.G);
-    };
-    KryVectors kv{};
-    kv.n = n;
-    kv.mask = h.mask.as<uint32_t>();
-    kv.r = vec(0);
-    kv.rhat = vec(1);
-    kv.p = vec(2);
-    kv.v = vec(3);
-    kv.s = vec(4);
-    kv.t = vec(5);
-    kv.abar = h.abar.as<float>();
-    float* abar_p = h.kry_abar.as<float>();
-    float* abar_s = abar_p + n + CELL_PAD;
-    kv.abar_p = abar_p;
-    kv.abar_s = abar_s;
-    kv.sc = h.kry_sc.as<double>();
-    kv.red = reduce_of(h);
-    const int lam_prev = h.lam_storage;
-    h.lam_storage = LBM_STORE_F32;  // the seed writes FP32 into r
-    AdjState st;
-    CK(cudaEventRecord(h.ev0, h.stream));
-    const double n0 = seed(h, w, st, h.record.as<float>(), 1.0, kv.r);
-    h.lam_storage = lam_prev;
-    CK(cudaMemsetAsync(h.abar.p, 0, (size_t)n * 4, h.stream));
-    const int grid = grid_for(h);
-    const double r0 = n0 * (double)st.s0;  // |r_0| in stored units
-    double resid = n0 == 0 ? 0.0 : 1.0;
-    bool converged = (n0 == 0);
-    const int64_t cap = o.max_iterations > 0 ? o.max_iterations : 100000;
-    const int64_t check = std::max<int64_t>(1, std::min<int64_t>(o.check_every > 0 ? o.check_every / 2 : 5, 10));
-    int64_t applications = 0;
-    float ms_adj = 0;
-    auto apply = [&](const float* in, float* out, const float* rhat, float* abar_out, double* dots) {
-        AdjArgs a = adj_args(h);
-        a.src = in;
-        a.dst = out;
-        a.record = h.record.as<float>();
-        a.rec_planes = 4;
-        a.ports = ports_at(h, h.t);
-        a.port_transpose = 1;
-        a.overwrite_abar = 1;
-        a.abar = abar_out;
-        a.in_scale_inv = 1.f;
-        a.out_scale = 1.f;
-        a.abar_factor = 1.f;
-        a.norm2 = nullptr;
-        a.kry = 1;
-        a.kry_rhat = rhat;
-        a.kry_dots = dots;
-        CK(launch_adjoint(h.Q, coll_kernel(h), LBM_STORE_F32, a, grid, h.stream));
-        ++applications;
-    };
-    if (!converged) {
-        cudaEvent_t e2, e3;
-        CK(cudaEventCreate(&e2));
-        CK(cudaEventCreate(&e3));
-        CK(cudaEventRecord(e2, h.stream));
-        CK(launch_krylov(h.Q, KRY_INIT, kv, grid, h.stream));
-        int64_t it = 0;
-        while (applications + 2 <= cap) {
-            apply(kv.p, kv.v, kv.rhat, abar_p, kv.sc + SC_K1);   // v = (I - L) p
-            CK(launch_krylov(h.Q, KRY_S, kv, grid, h.stream));   // s = r - alpha v
-            apply(kv.s, kv.t, nullptr, abar_s, kv.sc + SC_K3);   // t = (I - L) s
-            CK(launch_krylov(h.Q, KRY_R, kv, grid, h.stream));   // r = s - omega t, abar
-            ++it;
-            if (it % check == 0 || applications + 2 > cap) {
-                double rr[2];
-                CK(cudaMemcpyAsync(rr, kv.sc + SC_KR + 2, sizeof(rr), cudaMemcpyDeviceToHost, h.stream));
-                CK(cudaStreamSynchronize(h.stream));
-                resid = std::sqrt(std::max(0.0, rr[0] + rr[1])) / r0;
-                if (!std::isfinite(resid)) break;
-                if (resid <= o.tolerance) {
-                    converged = true;
-                    break;
-                }
-            }
-            CK(launch_krylov(h.Q, KRY_P, kv, grid, h.stream));   // p = r + beta (p - omega v)
-        }
-        CK(cudaEventRecord(e3, h.stream));
-        CK(cudaEventSynchronize(e3));
-        CK(cudaEventElapsedTime(&ms_adj, e2, e3));
-        cudaEventDestroy(e2);
-        cudaEventDestroy(e3);
-    }
-    check_errflag(h);
-    cudaEvent_t e4;
-    CK(cudaEventCreate(&e4));
-    CK(cudaEventRecord(e4, h.stream));
-    finish_gradient(h, st, applications > 0, grad);
-    float ms_sens = 0;
-    CK(cudaEventRecord(h.ev1, h.stream));
-    CK(cudaEventSynchronize(h.ev1));
-    CK(cudaEventElapsedTime(&ms_sens, e4, h.ev1));
-    cudaEventDestroy(e4);
-    if (rep) {
-        rep->residual = resid;
-        rep->iterations = applications;
-        rep->forward_recomputed = 0;
-        rep->peak_state_bytes = (int64_t)(h.record.bytes + h.kry.bytes + h.kry_abar.bytes);
-        rep->converged = converged ? 1 : 0;
-        rep->forward_ms = 0;
-        rep->adjoint_ms = ms_adj;
-        rep->sensitivity_ms = ms_sens;
-    }
-    if (!converged)
-        throw ConvergenceError("steady adjoint (BiCGStab) did not reach the residual tolerance within max_iterations "
-                               "(residual=" + repr_float(resid) + ")");
     return LBM_OK;
 }
 
@@ -2180,8 +2049,6 @@ lbm_status lbm_gradient(lbm_handle* h, const double* weights, const lbm_adjoint_
                                 "time_average");
         if (o.mode == LBM_ADJ_STEADY) {
             if (!(o.tolerance > 0)) throw ContractError("steady adjoint tolerance must be positive");
-            if (o.steady_solver == LBM_STEADY_BICGSTAB) return gradient_steady_bicgstab(*h, weights, o, grad, report);
-            if (o.steady_solver != LBM_STEADY_NEUMANN) throw ContractError("steady_solver must be neumann or bicgstab");
             return gradient_steady(*h, weights, o, grad, report);
         }
         if (o.mode != LBM_ADJ_HORIZON) throw ContractError("adjoint mode must be horizon or steady");

@@ -101,6 +101,7 @@ class SolverOptions:
     tolerance: float = 1e-8
     max_iterations: int = 100000
     time_average: bool = False        # also evaluate the responses of every state (stage objective)
+    collision_arithmetic: str = "float32"  # "float64": FP64 collision on FP32 storage
 
     @classmethod
     def parse(cls, v: Any) -> "SolverOptions":
@@ -109,10 +110,15 @@ class SolverOptions:
             return o
         if not isinstance(v, dict):
             raise _err("solver_options must be a mapping")
-        known = {"lattice", "collision", "population_storage", "filter", "adjoint", "time_average"}
+        known = {"lattice", "collision", "population_storage", "filter", "adjoint", "time_average",
+                 "collision_arithmetic"}
         if set(v) - known:
-            raise _err("solver_options accepts lattice, collision, population_storage, filter, adjoint and "
-                       "time_average")
+            raise _err("solver_options accepts lattice, collision, population_storage, filter, adjoint, "
+                       "time_average and collision_arithmetic")
+        ca = v.get("collision_arithmetic", "float32")
+        if ca not in ("float32", "float64"):
+            raise _err("solver_options.collision_arithmetic must be float32 or float64")
+        o.collision_arithmetic = ca
         ta = v.get("time_average", False)
         if not isinstance(ta, bool):
             raise _err("solver_options.time_average must be a boolean")
@@ -240,6 +246,7 @@ class NormalizedProblem:
             ports[k].ramp_s = port.get("ramp_s", 0.0)
         p.n_ports = len(self.ports)
         p.time_average = 1 if o.time_average else 0
+        p.collision_fp64 = 1 if o.collision_arithmetic == "float64" else 0
         p.ports = C.cast(ports, C.POINTER(_abi.Port))
         self._keep = [ports, p]
         return p

@@ -252,15 +252,12 @@ class LbmSolver:
         record_budget_bytes: int = 0,
         checkpointing: str = "every",
         snapshots: int = 0,
-        steady_solver: str = "neumann",
     ) -> tuple[np.ndarray, AdjointReport]:
         """Design gradient of w . responses: of the final state (objective
         "final") or of their mean over the horizon's states ("time_average",
         horizon mode, problems with solver_options.time_average).  Horizon
         checkpointing is a state every `checkpoint_every` steps ("every") or
-        the binomial schedule over `snapshots` states ("binomial").  The
-        steady adjoint sums the Neumann series ("neumann") or runs BiCGStab
-        ("bicgstab", float32 lambda storage)."""
+        the binomial schedule over `snapshots` states ("binomial")."""
         w = np.zeros(_abi.N_RESPONSES)
         w[: len(weights)] = np.asarray(weights, dtype=float)
         o = _abi.AdjointOpts()
@@ -276,7 +273,6 @@ class LbmSolver:
         o.checkpointing = _choice("checkpointing", checkpointing,
                                   {"every": _abi.LBM_CKPT_EVERY, "binomial": _abi.LBM_CKPT_BINOMIAL})
         o.snapshots = int(snapshots)
-        o.steady_solver = _choice("steady_solver", steady_solver, {"neumann": 0, "bicgstab": 1})
         grad = np.empty(self.shape)
         rep = _abi.AdjointReport()
         st = self.lib.lbm_gradient(self.h, _dp(w), C.byref(o), _dp(grad), C.byref(rep))

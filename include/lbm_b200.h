@@ -176,6 +176,13 @@ typedef struct {
      * t = 1..steps (lbm_time_average), and lbm_gradient accepts
      * LBM_OBJ_TIME_AVERAGE */
     int32_t time_average;
+    /* nonzero: the forward steps collide in FP64 arithmetic (FP32 storage
+     * only; no reference counterpart, the reference is FP64 throughout).
+     * FP32 collision arithmetic rounds the equilibrium momentum coherently
+     * over a nearly uniform flow, which biases the steady pressure by ~1e-7
+     * in density; FP64 collision removes that bias at ~1.6x the forward
+     * step's time.  The adjoint is FP32 in both cases. */
+    int32_t collision_fp64;
 } lbm_problem_t;
 
 /* Trajectory admission record (solver.rs:708-793).  Filled by lbm_forward
@@ -217,14 +224,6 @@ typedef enum { LBM_OBJ_FINAL = 0, LBM_OBJ_TIME_AVERAGE = 1 } lbm_objective;
  * minimises the recomputed steps for that number of states. */
 typedef enum { LBM_CKPT_EVERY = 0, LBM_CKPT_BINOMIAL = 1 } lbm_checkpointing;
 
-/* Solver of the STEADY adjoint (I - L) x = s, L the transposed step at the
- * final state (implexity-ad/src/implicit.rs:49-67 leaves the linear solve to
- * the provider).  NEUMANN sums the series sum_k L^k s (any lambda_storage);
- * BICGSTAB runs BiCGStab on the device with six FP32 vectors of the adjoint's
- * size (lambda_storage must be float32) and counts two operator applications
- * per iteration.  Both stop at |residual| <= tolerance |s|. */
-typedef enum { LBM_STEADY_NEUMANN = 0, LBM_STEADY_BICGSTAB = 1 } lbm_steady_solver;
-
 typedef struct {
     int32_t mode;             /* lbm_adjoint_mode */
     int32_t lambda_storage;   /* lbm_storage of the adjoint populations */
@@ -236,12 +235,11 @@ typedef struct {
     int32_t objective;        /* lbm_objective */
     int32_t checkpointing;    /* HORIZON: lbm_checkpointing */
     int64_t snapshots;        /* HORIZON, BINOMIAL: state slots (>= 1) */
-    int32_t steady_solver;    /* STEADY: lbm_steady_solver (0 = NEUMANN) */
 } lbm_adjoint_opts_t;
 
 typedef struct {
     double residual;              /* STEADY: final relative residual */
-    int64_t iterations;           /* adjoint steps taken (operator applications) */
+    int64_t iterations;           /* adjoint steps taken */
     int64_t forward_recomputed;   /* forward steps re-run from checkpoints */
     int64_t peak_state_bytes;     /* checkpoint + record bytes held on device */
     int32_t converged;

@@ -41,7 +41,18 @@ def test_oracle_fd_at_step_1e4_matches_gpu_adjoint(gpu_lib):
         s.forward()  # the horizon adjoint's recomputation leaves the state elsewhere
         g_s, rep = s.gradient(w, mode="steady", tolerance=1e-10)
     assert rep.converged
-    assert abs(J - float(fx["objective"])) <= 1e-6 * abs(float(fx["objective"]))
+    J_ref = float(fx["objective"])
+    # FP32 collision arithmetic: the coherent-rounding floor of the steady
+    # pressure (tests/test_scale_parity.py); FP64 collision arithmetic: the
+    # specification's 1e-6
+    assert abs(J - J_ref) <= 1e-5 * abs(J_ref)
+    prob64 = m.fd_problem()
+    prob64["solver_options"]["collision_arithmetic"] = "float64"
+    with LbmSolver(normalize(prob64)) as s64:
+        s64.set_design(raw)
+        s64.forward()
+        J64 = float(np.dot(w, s64.responses()))
+    assert abs(J64 - J_ref) <= 1e-6 * abs(J_ref), abs(J64 - J_ref) / abs(J_ref)
     dirs = list(directions(raw, editable, len(fx["seeds"]), int(fx["seeds"][0]), float(fx["fd_step"])))
     for k, (seed, d) in enumerate(dirs):
         assert seed == int(fx["seeds"][k])
