@@ -47,6 +47,8 @@ EXPORTS = [
     "lbm_fields",
     "lbm_gradient",
     "lbm_step_vjp",
+    "lbm_step_vjp_tau",
+    "lbm_set_tau",
     "lbm_design_vjp",
     "lbm_state_stats_noalloc",
 ]
@@ -184,6 +186,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.lbm_fields.argtypes = [h, _dp, _dp, _dp]
     lib.lbm_gradient.argtypes = [h, _dp, C.POINTER(AdjointOpts), _dp, C.POINTER(AdjointReport)]
     lib.lbm_step_vjp.argtypes = [h, _dp, _dp, _dp, _dp, C.c_size_t]
+    lib.lbm_step_vjp_tau.argtypes = [h, _dp, _dp, _dp, _dp, _dp, C.c_size_t]
+    lib.lbm_set_tau.argtypes = [h, _dp, C.c_size_t]
     lib.lbm_design_vjp.argtypes = [h, _dp, _dp, C.c_size_t]
     lib.lbm_state_stats_noalloc.argtypes = [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, _dp,
                                             C.c_void_p, C.c_void_p]

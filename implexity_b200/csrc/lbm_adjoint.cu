@@ -115,7 +115,9 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
                 const float rp = st->rec[0][a.recd[0] + c];
                 // v stays in the stored scale (the transposed step is linear): the
                 // alpha cotangent is rescaled once, the output by out_scale / in_scale
-                float ab = collide_vjp<Q, COLL>(v, rp, u, st->alpha[c], a.P) * a.in_scale_inv;
+                float om = a.P.omega, omm = a.P.om;
+                if (a.omega_cell) om = omm = a.omega_cell[x];  // Tau::PerCell (BGK only)
+                float ab = collide_vjp<Q, COLL>(v, rp, u, st->alpha[c], a.P, om, omm) * a.in_scale_inv;
                 if constexpr (STG) {
                     if (a.stage) {
                         // the stage seed of this state: d(w . responses)/dg from its record

@@ -342,7 +342,8 @@ __device__ __forceinline__ float dotc(int q, const float (&v)[3]) {
 // (rho - 1)(sum w - 1) per cell and step -- systematic where the pressure
 // has one sign.
 template <int Q, int COLL, int SC>
-__device__ __forceinline__ Macro collide_fused(float (&v)[Q], float alpha, const Physics& P, bool post) {
+__device__ __forceinline__ Macro collide_fused(float (&v)[Q], float alpha, const Physics& P, bool post, float om,
+                                              float omm) {
     using L = Lat<Q>;
     constexpr int NP = L::NPAIR;
     float S[NP], D[NP];
@@ -373,7 +374,6 @@ __device__ __forceinline__ Macro collide_fused(float (&v)[Q], float alpha, const
     for (int d = 0; d < 3; ++d) M.F[d] = M.rho * (P.a[d] - alpha * M.u[d]);
     if (!post) return M;
 
-    const float om = P.omega, omm = P.om;
     const float kp = 1.f - 0.5f * om, km = 1.f - 0.5f * omm;
     const float hp = 0.5f * (1.f - om), hm = 0.5f * (1.f - omm);
     const float rho = M.rho;
@@ -504,7 +504,8 @@ __device__ __forceinline__ Macro collide_fused(float (&v)[Q], float alpha, const
 // alone leaves ~1e-9.  Selected per problem (collision_fp64); the rates and
 // MRT basis vectors are the FP32 ones of Physics.
 template <int Q, int COLL>
-__device__ __forceinline__ Macro collide_fused_dp(float (&vf)[Q], float alpha_f, const Physics& P, bool post) {
+__device__ __forceinline__ Macro collide_fused_dp(float (&vf)[Q], float alpha_f, const Physics& P, bool post,
+                                                 float om_f, float omm_f) {
     using L = Lat<Q>;
     constexpr int NP = L::NPAIR;
     double v[Q];
@@ -538,7 +539,7 @@ __device__ __forceinline__ Macro collide_fused_dp(float (&vf)[Q], float alpha_f,
         M.F[d] = (float)F[d];
     }
     if (!post) return M;
-    const double om = P.omega, omm = P.om;
+    const double om = om_f, omm = omm_f;
     const double kp = 1.0 - 0.5 * om, km = 1.0 - 0.5 * omm;
     const double hp = 0.5 * (1.0 - om), hm = 0.5 * (1.0 - omm);
     const double usq15 = 1.5 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
@@ -622,10 +623,9 @@ __device__ __forceinline__ Macro collide_fused_dp(float (&vf)[Q], float alpha_f,
 // Brinkman chain F = rho (a - alpha u), u = (m/rho + a/2)/(1 + alpha/2).
 template <int Q, int COLL>
 __device__ __forceinline__ float collide_vjp(float (&gb)[Q], float rp, const float (&u)[3], float alpha,
-                                             const Physics& P) {
+                                             const Physics& P, float om, float omm) {
     using L = Lat<Q>;
     constexpr int NP = L::NPAIR;
-    const float om = P.omega, omm = P.om;
     const float rho = 1.f + rp;
     const float s = 1.f + 0.5f * alpha;
     float F[3];

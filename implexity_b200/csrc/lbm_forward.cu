@@ -157,9 +157,12 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
                         for (int e = 0; e < 6; ++e) a.record[(size_t)(4 + e) * n + x] = S[e];
                     }
                 }
+                // relaxation rates: the problem's, or the cell's own (Tau::PerCell, BGK only)
+                float om = a.P.omega, omm = a.P.om;
+                if (a.omega_cell) om = omm = a.omega_cell[x];
                 Macro M;
-                if constexpr (DP) M = collide_fused_dp<Q, COLL>(v, alpha, a.P, a.collide);
-                else M = collide_fused<Q, COLL, SC>(v, alpha, a.P, a.collide);
+                if constexpr (DP) M = collide_fused_dp<Q, COLL>(v, alpha, a.P, a.collide, om, omm);
+                else M = collide_fused<Q, COLL, SC>(v, alpha, a.P, a.collide, om, omm);
                 if constexpr (RSP) {
                     float r6[6];
                     response_cell<Q>(M.rp, M.u, S, alpha, a.sp, a.P, r6);

@@ -51,6 +51,7 @@ struct FwdArgs {
     int64_t run0[27];
     int32_t rund[27];
     int32_t dp_collision;    // FP64 collision arithmetic (FP32 storage)
+    const float* omega_cell; // per-cell relaxation rate 1/tau (BGK; nullptr: the uniform rate of P)
 };
 
 struct AdjArgs {
@@ -78,6 +79,7 @@ struct AdjArgs {
     int32_t rund[27];
     int64_t rec0[10];        // staged record runs
     int32_t recd[10];
+    const float* omega_cell; // per-cell relaxation rate 1/tau (BGK; nullptr: the uniform rate of P)
 };
 
 struct ObjArgs {
@@ -155,7 +157,13 @@ cudaError_t launch_upload_pop(int Q, int storage, const Geometry& G, void* pop, 
 cudaError_t launch_wall_loads(int Q, int storage, const Geometry& G, const Physics& P, const void* A,
                               const uint32_t* mask, const float* alpha, const PortMap* ports, int apply_ports,
                               const uint32_t* cells, const uint8_t* links, int64_t n_links, double* out,
-                              cudaStream_t s);
+                              const float* omega_cell, cudaStream_t s);
+// Per-cell cotangent of the relaxation time of one step (interval_vjp with
+// Tau::PerCell, solver.rs:214-285 tau_bar): g = canonical populations g = f - w
+// of the state, lam = the stored cotangent of the next state (FP32).
+cudaError_t launch_tau_bar(int Q, const Geometry& G, const Physics& P, const float* g, const float* lam,
+                           const uint32_t* mask, const float* alpha, const float* omega_cell, double* out, int grid,
+                           cudaStream_t s);
 cudaError_t launch_canon_lam(int Q, int lstorage, const Geometry& G, const void* lam, const uint32_t* mask,
                              float inv_scale, float* out, int grid, cudaStream_t s);
 cudaError_t launch_seed_lam(int Q, int lstorage, const Geometry& G, void* lam, const uint32_t* mask,

@@ -249,7 +249,7 @@ template <int Q, typename T>
 __global__ void __launch_bounds__(BLOCK) k_wall_loads(Geometry G, Physics P, const T* A, const uint32_t* __restrict__ mask,
                                                       const float* __restrict__ alpha, const PortMap* ports,
                                                       int apply_ports, const uint32_t* cells, const uint8_t* links,
-                                                      int64_t n_links, double* out) {
+                                                      int64_t n_links, double* out, const float* omega_cell) {
     for (int64_t i = (int64_t)blockIdx.x * BLOCK + threadIdx.x; i < n_links; i += (int64_t)gridDim.x * BLOCK) {
         const uint32_t x = cells[i];
         const int q = links[i];
@@ -257,12 +257,64 @@ __global__ void __launch_bounds__(BLOCK) k_wall_loads(Geometry G, Physics P, con
         float g[Q];
         load_pop<Q, T>(A, G, x, m, g);
         if (apply_ports && (m & MASK_PORT)) apply_port<Q>(ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], g);
-        collide_fused<Q, CK_PAIRS, 0>(g, alpha[x], P, true);
+        const float om = omega_cell ? omega_cell[x] : P.omega;  // BGK: both pair rates
+        collide_fused<Q, CK_PAIRS, 0>(g, alpha[x], P, true, om, om);
         float o = 0.f;
 #pragma unroll
         for (int r = 0; r < Q; ++r)
             if (r == opp<Q>(q)) o = g[r];
         out[i] = (double)o;
+    }
+}
+
+// ------------------------------------------------------------------ relaxation-time cotangent
+// tau_bar of interval_vjp with Tau::PerCell (collide_cell_vjp, solver.rs:
+// 214-285): with post_bar the cotangent of the cell's post-collision
+// populations (gathered from the stored next-state cotangent like the
+// transposed step), tau_bar = sum_q post_bar_q [(f_q - eq_q) + w_q (3 c.F -
+// 3 u.F + 9 (c.u)(c.F)) / 2] / tau^2 at the state f.  FP64 arithmetic; one
+// thread per cell (a per-step call, not a stepping kernel).
+template <int Q>
+__global__ void __launch_bounds__(BLOCK) k_tau_bar(Geometry G, Physics P, const float* __restrict__ g,
+                                                   const float* __restrict__ lam, const uint32_t* __restrict__ mask,
+                                                   const float* __restrict__ alpha,
+                                                   const float* __restrict__ omega_cell, double* out) {
+    using L = Lat<Q>;
+    const uint32_t n = (uint32_t)G.n;
+    for (uint32_t x = blockIdx.x * BLOCK + threadIdx.x; x < n; x += gridDim.x * BLOCK) {
+        const uint32_t m = mask[x];
+        if (m & MASK_SOLID) {
+            out[x] = 0.0;
+            continue;
+        }
+        double f[Q], rho = 0.0, j[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            f[q] = L::wd(q) + (double)g[(size_t)q * n + x];
+            rho += f[q];
+            j[0] += L::cx(q) * f[q];
+            j[1] += L::cy(q) * f[q];
+            j[2] += L::cz(q) * f[q];
+        }
+        const double al = alpha[x], s = 1.0 + 0.5 * al;
+        double u[3], F[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            u[d] = (j[d] / rho + 0.5 * (double)P.a[d]) / s;
+            F[d] = rho * ((double)P.a[d] - al * u[d]);
+        }
+        const double usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+        const double uf = u[0] * F[0] + u[1] * F[1] + u[2] * F[2];
+        const double tau = 1.0 / (double)(omega_cell ? omega_cell[x] : P.omega);
+        double tb = 0.0;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const double pb = (double)lam[pull_adj_index<Q>(G, x, m, q)];
+            const double cu = dotc_d<Q>(q, u), cf = dotc_d<Q>(q, F);
+            const double eq = rho * L::wd(q) * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * usq);
+            tb += pb * ((f[q] - eq) + 0.5 * L::wd(q) * (3.0 * cf - 3.0 * uf + 9.0 * cu * cf));
+        }
+        out[x] = tb / (tau * tau);
     }
 }
 
@@ -451,7 +503,7 @@ cudaError_t launch_upload_pop(int Q, int storage, const Geometry& G, void* pop, 
 cudaError_t launch_wall_loads(int Q, int storage, const Geometry& G, const Physics& P, const void* A,
                               const uint32_t* mask, const float* alpha, const PortMap* ports, int apply_ports,
                               const uint32_t* cells, const uint8_t* links, int64_t n_links, double* out,
-                              cudaStream_t s) {
+                              const float* omega_cell, cudaStream_t s) {
     if (n_links <= 0) return cudaSuccess;
     const int grid = (int)std::min<int64_t>((n_links + BLOCK - 1) / BLOCK, 4096);
     Physics B = P;
@@ -460,13 +512,21 @@ cudaError_t launch_wall_loads(int Q, int storage, const Geometry& G, const Physi
         LBM_STORAGE_DISPATCH(storage, T,
                              k_wall_loads<19, T><<<grid, BLOCK, 0, s>>>(G, B, static_cast<const T*>(A), mask, alpha,
                                                                          ports, apply_ports, cells, links, n_links,
-                                                                         out))
+                                                                         out, omega_cell))
     } else {
         LBM_STORAGE_DISPATCH(storage, T,
                              k_wall_loads<27, T><<<grid, BLOCK, 0, s>>>(G, B, static_cast<const T*>(A), mask, alpha,
                                                                          ports, apply_ports, cells, links, n_links,
-                                                                         out))
+                                                                         out, omega_cell))
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tau_bar(int Q, const Geometry& G, const Physics& P, const float* g, const float* lam,
+                           const uint32_t* mask, const float* alpha, const float* omega_cell, double* out, int grid,
+                           cudaStream_t s) {
+    if (Q == 19) k_tau_bar<19><<<grid, BLOCK, 0, s>>>(G, P, g, lam, mask, alpha, omega_cell, out);
+    else k_tau_bar<27><<<grid, BLOCK, 0, s>>>(G, P, g, lam, mask, alpha, omega_cell, out);
     return cudaGetLastError();
 }
 

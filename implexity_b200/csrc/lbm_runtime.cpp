@@ -322,6 +322,8 @@ struct lbm_handle {
     // --- normalised problem
     int Q = 19, coll = LBM_BGK, storage = LBM_STORE_F32;
     bool collision_fp64 = false;  // FP64 collision arithmetic on FP32 storage
+    // Tau::PerCell (solver.rs:171-187): per-cell rates 1/tau of the BGK collision (FP32), when set
+    bool tau_per_cell = false;
     Geometry G{};
     Physics P{};
     HostLat L{};
@@ -341,6 +343,7 @@ struct lbm_handle {
     int64_t device_bytes = 0;
     DevBuf pop, mask, alpha, phi, raw, den, slope, cls_d, fixed_d, offsets_d, ports_d, partial, counter, diag;
     DevBuf lam, record, abar, abar_final, phibar, scale, grad, norm2, sums, scratch, errflag;
+    DevBuf omega_cell, tau_state, tau_bar;
     int lam_storage = LBM_STORE_F32;
     // --- ports: normalised specs with their signals; pulsatile ports keep one
     // set of maps per state index on the device (ensure_port_maps)
@@ -837,6 +840,7 @@ FwdArgs fwd_args(lbm_handle& h) {
     a.sp.dt_s = (float)h.dt;
     a.sp.tau = (float)h.tau;
     a.dp_collision = h.collision_fp64 ? 1 : 0;
+    a.omega_cell = h.tau_per_cell ? h.omega_cell.as<float>() : nullptr;
     return a;
 }
 
@@ -1127,6 +1131,7 @@ AdjArgs adj_args(lbm_handle& h) {
     a.abar = h.abar.as<float>();
     a.red = reduce_of(h);
     a.err = h.errflag.as<int>();
+    a.omega_cell = h.tau_per_cell ? h.omega_cell.as<float>() : nullptr;
     return a;
 }
 
@@ -1787,6 +1792,32 @@ lbm_status lbm_set_design(lbm_handle* h, const double* raw, size_t n) {
     });
 }
 
+lbm_status lbm_set_tau(lbm_handle* h, const double* tau, size_t n) {
+    return guarded(h, [&]() {
+        if (!tau) {
+            h->tau_per_cell = false;
+            h->forward_done = false;
+            return LBM_OK;
+        }
+        if (h->coll != LBM_BGK)
+            throw ContractError("per-cell relaxation times need the BGK collision (Tau::PerCell of the density-design "
+                                "solver)");
+        check_n(*h, n, (size_t)h->n(), "tau");
+        std::vector<float> om(n);
+        for (size_t x = 0; x < n; ++x) {
+            if (!std::isfinite(tau[x]) || !(tau[x] > 0.5))
+                throw ContractError("per-cell relaxation times must be finite and greater than 0.5");
+            om[x] = (float)(1.0 / tau[x]);
+        }
+        h->omega_cell.alloc((n + CELL_PAD) * sizeof(float), &h->device_bytes);
+        CK(cudaMemcpyAsync(h->omega_cell.p, om.data(), n * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        h->tau_per_cell = true;
+        h->forward_done = false;
+        return LBM_OK;
+    });
+}
+
 lbm_status lbm_get_design(lbm_handle* h, double* phi, double* alpha) {
     return guarded(h, [&]() {
         require_design(*h);
@@ -1933,7 +1964,8 @@ lbm_status lbm_wall_loads(lbm_handle* h, double pressure_datum_pa, const double*
             const void* prev = h->pop_array(h->cur ^ 1) + pop_pad(h->G) * storage_bytes(h->storage);
             CK(launch_wall_loads(h->Q, h->storage, h->G, h->P, prev, h->mask.as<uint32_t>(), h->alpha.as<float>(),
                                  ports_at(*h, tb), (tb >= 1 && h->n_ports > 0) ? 1 : 0, h->wall_cells_d.as<uint32_t>(),
-                                 h->wall_links_d.as<uint8_t>(), (int64_t)nl, h->wall_out.as<double>(), h->stream));
+                                 h->wall_links_d.as<uint8_t>(), (int64_t)nl, h->wall_out.as<double>(),
+                                 h->tau_per_cell ? h->omega_cell.as<float>() : nullptr, h->stream));
         }
         std::vector<double> g(nl);
         if (nl > 0) CK(cudaMemcpyAsync(g.data(), h->wall_out.p, nl * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -2061,47 +2093,80 @@ lbm_status lbm_gradient(lbm_handle* h, const double* weights, const lbm_adjoint_
     });
 }
 
+namespace {
+// interval_vjp (solver.rs:642-674) of one step from a host state: the
+// cotangent of the state, of alpha and (tau_bar != NULL) of the per-cell
+// relaxation times.
+lbm_status step_vjp_impl(lbm_handle* h, const double* state, const double* lambda_next, double* lambda,
+                         double* alpha_bar, double* tau_bar, size_t n_populations) {
+    require_design(*h);
+    const int64_t N = h->n();
+    const int Q = h->Q;
+    check_n(*h, n_populations, (size_t)(N * Q), "populations");
+    lbm_status s = lbm_set_populations(h, state, n_populations);
+    if (s != LBM_OK) throw ContractError(h->err);
+    int64_t* ctr = &h->device_bytes;
+    if (tau_bar) {
+        // lbm_set_populations left the state's g = f - w planes in the scratch array
+        h->tau_state.alloc((size_t)N * Q * sizeof(float), ctr);
+        CK(cudaMemcpyAsync(h->tau_state.p, h->scratch.p, (size_t)N * Q * sizeof(float), cudaMemcpyDeviceToDevice,
+                           h->stream));
+        h->tau_bar.alloc((size_t)N * sizeof(double), ctr);
+    }
+    alloc_adjoint(*h, LBM_STORE_F32);
+    h->record.alloc(((size_t)N * 4 + CELL_PAD) * sizeof(float), ctr);
+    inspect(*h, nullptr, h->record.as<float>());
+    std::vector<float> v((size_t)N * Q);
+    for (int64_t x = 0; x < N; ++x)
+        for (int q = 0; q < Q; ++q) v[(size_t)q * N + x] = (float)lambda_next[x * Q + q];
+    ensure_scratch(*h);
+    CK(cudaMemcpyAsync(h->scratch.p, v.data(), v.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(launch_seed_lam(Q, LBM_STORE_F32, h->G, h->lamA(), h->mask.as<uint32_t>(), ports_at(*h, h->t + 1),
+                       h->scratch.as<float>(), 1.f, 1, grid_for(*h), h->stream));
+    if (tau_bar)
+        CK(launch_tau_bar(Q, h->G, h->P, h->tau_state.as<float>(), static_cast<const float*>(h->lamA()),
+                          h->mask.as<uint32_t>(), h->alpha.as<float>(),
+                          h->tau_per_cell ? h->omega_cell.as<float>() : nullptr, h->tau_bar.as<double>(),
+                          grid_for(*h), h->stream));
+    AdjArgs a = adj_args(*h);
+    a.record = h->record.as<float>();
+    a.port_transpose = 0;
+    a.overwrite_abar = 1;
+    a.in_scale_inv = 1.f;
+    a.out_scale = 1.f;
+    a.abar_factor = 1.f;
+    CK(launch_adjoint(Q, coll_kernel(*h), LBM_STORE_F32, a, grid_for(*h), h->stream));
+    h->lcur ^= 1;
+    check_errflag(*h);
+    CK(launch_canon_lam(Q, LBM_STORE_F32, h->G, h->lamA(), h->mask.as<uint32_t>(), 1.f, h->scratch.as<float>(),
+                        grid_for(*h), h->stream));
+    CK(cudaMemcpyAsync(v.data(), h->scratch.p, v.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+    std::vector<float> ab((size_t)N);
+    CK(cudaMemcpyAsync(ab.data(), h->abar.p, ab.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (tau_bar)
+        CK(cudaMemcpyAsync(tau_bar, h->tau_bar.p, (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int64_t x = 0; x < N; ++x) {
+        for (int q = 0; q < Q; ++q) lambda[x * Q + q] = v[(size_t)q * N + x];
+        if (alpha_bar) alpha_bar[x] = h->cls[x] == 0 ? 0.0 : (double)ab[x];
+    }
+    return LBM_OK;
+}
+}  // namespace
+
 lbm_status lbm_step_vjp(lbm_handle* h, const double* state, const double* lambda_next, double* lambda,
                         double* alpha_bar, size_t n_populations) {
+    return guarded(h, [&]() { return step_vjp_impl(h, state, lambda_next, lambda, alpha_bar, nullptr, n_populations); });
+}
+
+lbm_status lbm_step_vjp_tau(lbm_handle* h, const double* state, const double* lambda_next, double* lambda,
+                            double* alpha_bar, double* tau_bar, size_t n_populations) {
     return guarded(h, [&]() {
-        require_design(*h);
-        const int64_t N = h->n();
-        const int Q = h->Q;
-        check_n(*h, n_populations, (size_t)(N * Q), "populations");
-        lbm_status s = lbm_set_populations(h, state, n_populations);
-        if (s != LBM_OK) throw ContractError(h->err);
-        int64_t* ctr = &h->device_bytes;
-        alloc_adjoint(*h, LBM_STORE_F32);
-        h->record.alloc(((size_t)N * 4 + CELL_PAD) * sizeof(float), ctr);
-        inspect(*h, nullptr, h->record.as<float>());
-        std::vector<float> v((size_t)N * Q);
-        for (int64_t x = 0; x < N; ++x)
-            for (int q = 0; q < Q; ++q) v[(size_t)q * N + x] = (float)lambda_next[x * Q + q];
-        ensure_scratch(*h);
-        CK(cudaMemcpyAsync(h->scratch.p, v.data(), v.size() * 4, cudaMemcpyHostToDevice, h->stream));
-        CK(launch_seed_lam(Q, LBM_STORE_F32, h->G, h->lamA(), h->mask.as<uint32_t>(), ports_at(*h, h->t + 1),
-                           h->scratch.as<float>(), 1.f, 1, grid_for(*h), h->stream));
-        AdjArgs a = adj_args(*h);
-        a.record = h->record.as<float>();
-        a.port_transpose = 0;
-        a.overwrite_abar = 1;
-        a.in_scale_inv = 1.f;
-        a.out_scale = 1.f;
-        a.abar_factor = 1.f;
-        CK(launch_adjoint(Q, coll_kernel(*h), LBM_STORE_F32, a, grid_for(*h), h->stream));
-        h->lcur ^= 1;
-        check_errflag(*h);
-        CK(launch_canon_lam(Q, LBM_STORE_F32, h->G, h->lamA(), h->mask.as<uint32_t>(), 1.f, h->scratch.as<float>(),
-                            grid_for(*h), h->stream));
-        CK(cudaMemcpyAsync(v.data(), h->scratch.p, v.size() * 4, cudaMemcpyDeviceToHost, h->stream));
-        std::vector<float> ab((size_t)N);
-        CK(cudaMemcpyAsync(ab.data(), h->abar.p, ab.size() * 4, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        for (int64_t x = 0; x < N; ++x) {
-            for (int q = 0; q < Q; ++q) lambda[x * Q + q] = v[(size_t)q * N + x];
-            if (alpha_bar) alpha_bar[x] = h->cls[x] == 0 ? 0.0 : (double)ab[x];
-        }
-        return LBM_OK;
+        if (!tau_bar) throw ContractError("tau_bar must not be NULL");
+        if (h->coll != LBM_BGK)
+            throw ContractError("per-cell relaxation times need the BGK collision (Tau::PerCell of the density-design "
+                                "solver)");
+        return step_vjp_impl(h, state, lambda_next, lambda, alpha_bar, tau_bar, n_populations);
     });
 }
 

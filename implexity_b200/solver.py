@@ -298,6 +298,24 @@ class LbmSolver:
         self._check(self.lib.lbm_step_vjp(self.h, _dp(s), _dp(ln), _dp(lam), _dp(ab), s.size))
         return lam.reshape(self.cells, self.q), ab
 
+    def set_tau(self, tau: np.ndarray | None):
+        """Per-cell relaxation times (Tau::PerCell, BGK problems), or None for
+        the problem's uniform tau."""
+        if tau is None:
+            self._check(self.lib.lbm_set_tau(self.h, None, 0))
+            return
+        t = np.ascontiguousarray(tau, dtype=np.float64).reshape(-1)
+        self._check(self.lib.lbm_set_tau(self.h, _dp(t), t.size))
+
+    def step_vjp_tau(self, state: np.ndarray, lambda_next: np.ndarray):
+        """step_vjp plus the per-cell cotangent of the relaxation time."""
+        s = np.ascontiguousarray(state, dtype=np.float64).reshape(-1)
+        ln = np.ascontiguousarray(lambda_next, dtype=np.float64).reshape(-1)
+        lam = np.empty_like(s)
+        ab, tb = np.empty(self.cells), np.empty(self.cells)
+        self._check(self.lib.lbm_step_vjp_tau(self.h, _dp(s), _dp(ln), _dp(lam), _dp(ab), _dp(tb), s.size))
+        return lam.reshape(self.cells, self.q), ab, tb
+
     def design_vjp(self, phi_bar: np.ndarray) -> np.ndarray:
         pb = np.ascontiguousarray(phi_bar, dtype=np.float64).reshape(-1)
         out = np.empty(self.cells)

@@ -26,6 +26,8 @@
  *   lbm_set_populations / lbm_get_populations / lbm_advance
  *                     TimeStepper::{initial_state, advance}  implexity-solve/src/time_stepper.rs:81-148
  *   lbm_step_vjp      LbmProblem::interval_vjp     src/solver.rs:642-674
+ *   lbm_set_tau / lbm_step_vjp_tau
+ *                     Tau::PerCell                 src/solver.rs:171-187 (interval / interval_vjp)
  *
  * Conventions
  *   - Cells are indexed like the reference Grid: cell = (i*ny + j)*nz + k
@@ -283,6 +285,15 @@ LBM_API lbm_status lbm_info(const lbm_handle* h, lbm_info_t* out);
  * 284-286).  raw has N entries in [0,1]. */
 LBM_API lbm_status lbm_set_design(lbm_handle* h, const double* raw, size_t n);
 
+/* Per-cell relaxation times (Tau::PerCell, solver.rs:171-187), the form the
+ * reference's thermal provider steps with (thermal_provider.rs:616,1137):
+ * tau has N entries (lattice units, finite, > 0.5) and replaces the problem's
+ * uniform tau in the BGK collision of every forward step, transposed step
+ * and wall-load evaluation; NULL returns to the uniform tau.  BGK problems
+ * only.  The viscous-dissipation response keeps the problem's uniform tau.
+ * A forward run must follow before lbm_gradient. */
+LBM_API lbm_status lbm_set_tau(lbm_handle* h, const double* tau, size_t n);
+
 /* Copies the mapped fluid fraction phi and the Brinkman resistance alpha
  * (per time step) to the host (either pointer may be NULL). */
 LBM_API lbm_status lbm_get_design(lbm_handle* h, double* phi, double* alpha);
@@ -371,6 +382,13 @@ LBM_API lbm_status lbm_gradient(lbm_handle* h, const double* weights, const lbm_
  * populations cell-major.  alpha_bar may be NULL. */
 LBM_API lbm_status lbm_step_vjp(lbm_handle* h, const double* state, const double* lambda_next,
                         double* lambda, double* alpha_bar, size_t n_populations);
+
+/* lbm_step_vjp that also returns the per-cell cotangent of the relaxation
+ * time (interval_vjp's tau_bar with Tau::PerCell, solver.rs:214-285,
+ * 331-356, 642-674): tau_bar has N entries (0 at solid cells).  BGK
+ * problems only; the rates are those of lbm_set_tau (or the uniform tau). */
+LBM_API lbm_status lbm_step_vjp_tau(lbm_handle* h, const double* state, const double* lambda_next, double* lambda,
+                                    double* alpha_bar, double* tau_bar, size_t n_populations);
 
 /* Design-map transpose alone (DesignMap::vjp, design.rs:219-243) for the
  * design last set: out[N] = d phi / d raw ^T phi_bar. */

@@ -164,6 +164,9 @@ struct Row {
 
 struct orc_problem {
     Lattice L;
+    // Tau::PerCell (solver.rs:171-187): per-cell relaxation times of the BGK
+    // collision; empty = Tau::Uniform(tau)
+    std::vector<double> tau_cell;
     int Q = 19;
     int coll = LBM_BGK;
     int64_t shape[3] = {0, 0, 0};
@@ -394,24 +397,27 @@ inline void macroscopic(const orc_problem& o, const double* f, double alpha, dou
 }
 
 // Static-provider BGK (solver.rs:298-322).
-void collide_bgk(const orc_problem& o, const double* f, double alpha, double* out) {
+void collide_bgk(const orc_problem& o, const double* f, double alpha, double* out, double tau) {
     const Lattice& L = o.L;
     double rho, u[3], F[3];
     macroscopic(o, f, alpha, rho, u, F);
     double uf = u[0] * F[0] + u[1] * F[1] + u[2] * F[2];
     double usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-    double k = 1.0 - 0.5 / o.tau;
+    double k = 1.0 - 0.5 / tau;
     for (int q = 0; q < L.Q; ++q) {
         double cu = dotc(L, q, u), cf = dotc(L, q, F);
         double eq = rho * L.w[q] * (1.0 + cu * 3.0 + cu * cu * 4.5 - usq * 1.5);
         double src = k * L.w[q] * (cf * 3.0 - uf * 3.0 + cu * cf * 9.0);
-        out[q] = f[q] - (f[q] - eq) / o.tau + src;
+        out[q] = f[q] - (f[q] - eq) / tau + src;
     }
 }
 
-// collide_cell_vjp, solver.rs:214-285 (returns f_bar and alpha_bar).
+// The relaxation time of cell x (Tau::at, solver.rs:180-186).
+inline double tau_at(const orc_problem& o, int64_t x) { return o.tau_cell.empty() ? o.tau : o.tau_cell[x]; }
+
+// collide_cell_vjp, solver.rs:214-285 (returns f_bar, alpha_bar and tau_bar).
 void collide_bgk_vjp(const orc_problem& o, const double* f, double alpha, const double* g, double* f_bar,
-                     double& alpha_bar) {
+                     double& alpha_bar, double tau, double& tau_bar) {
     const Lattice& L = o.L;
     const int Q = L.Q;
     double rho, m[3];
@@ -421,9 +427,10 @@ void collide_bgk_vjp(const orc_problem& o, const double* f, double alpha, const 
     for (int d = 0; d < 3; ++d) u[d] = (m[d] / rho + 0.5 * o.a[d]) / s;
     for (int d = 0; d < 3; ++d) F[d] = rho * (o.a[d] - alpha * u[d]);
     double usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-    double tau = o.tau;
+    double uf = u[0] * F[0] + u[1] * F[1] + u[2] * F[2];
     double k = 1.0 - 0.5 / tau;
     double rho_bar = 0, uf_bar = 0, usq_bar = 0;
+    tau_bar = 0;
     double u_bar[3] = {0, 0, 0}, F_bar[3] = {0, 0, 0};
     for (int q = 0; q < Q; ++q) f_bar[q] = 0;
     for (int q = 0; q < Q; ++q) {
@@ -433,6 +440,9 @@ void collide_bgk_vjp(const orc_problem& o, const double* f, double alpha, const 
         double poly = 1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * usq;
         f_bar[q] += gq * (1.0 - 1.0 / tau);
         double eq_bar = gq / tau;
+        double eq = rho * L.w[q] * poly;
+        tau_bar += gq * (f[q] - eq) / (tau * tau) +
+                   gq * L.w[q] * (0.5 / (tau * tau)) * (3.0 * cf - 3.0 * uf + 9.0 * cu * cf);
         double h = gq * L.w[q] * k;
         double cf_bar = h * (3.0 + 9.0 * cu);
         double cu_bar = h * 9.0 * cf;
@@ -678,9 +688,9 @@ void collide_mrt_vjp(const orc_problem& o, const double* f, double rho, const do
 }
 
 // One cell update: collide of the selected operator.
-void collide_cell(const orc_problem& o, const double* f, double alpha, double* out) {
+void collide_cell(const orc_problem& o, const double* f, double alpha, double* out, double tau) {
     if (o.coll == LBM_BGK) {
-        collide_bgk(o, f, alpha, out);
+        collide_bgk(o, f, alpha, out, tau);
         return;
     }
     double rho, u[3], F[3];
@@ -692,9 +702,10 @@ void collide_cell(const orc_problem& o, const double* f, double alpha, double* o
 // Collision VJP with the Brinkman chain of moving/psm.rs cell_update_vjp
 // (Brinkman branch, zero solid velocity, :402-486).
 void collide_cell_vjp(const orc_problem& o, const double* f, double alpha, const double* g, double* f_bar,
-                      double& alpha_bar) {
+                      double& alpha_bar, double tau, double& tau_bar) {
+    tau_bar = 0;
     if (o.coll == LBM_BGK) {
-        collide_bgk_vjp(o, f, alpha, g, f_bar, alpha_bar);
+        collide_bgk_vjp(o, f, alpha, g, f_bar, alpha_bar, tau, tau_bar);
         return;
     }
     const Lattice& L = o.L;
@@ -744,7 +755,7 @@ double interval(const orc_problem& o, const double* before, const double* alpha,
     const int64_t N = o.N;
     post.resize((size_t)N * Q);
 #pragma omp parallel for schedule(static)
-    for (int64_t x = 0; x < N; ++x) collide_cell(o, before + x * Q, alpha[x], post.data() + x * Q);
+    for (int64_t x = 0; x < N; ++x) collide_cell(o, before + x * Q, alpha[x], post.data() + x * Q, tau_at(o, x));
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < N * Q; ++i) {
         uint32_t s = o.source[i];
@@ -767,7 +778,7 @@ double interval(const orc_problem& o, const double* before, const double* alpha,
 // interval_vjp, solver.rs:642-674, with apply_ports_vjp (ports.rs:582-621)
 // and Streaming::stream_vjp (solver.rs:138-157).
 void interval_vjp(const orc_problem& o, const double* before, const double* alpha, const double* after_bar,
-                  double* f_bar, double* alpha_bar) {
+                  double* f_bar, double* alpha_bar, double* tau_bar = nullptr) {
     const int Q = o.Q;
     const int64_t N = o.N;
     std::vector<double> refl(after_bar, after_bar + N * Q);
@@ -800,15 +811,16 @@ void interval_vjp(const orc_problem& o, const double* before, const double* alph
         const double* g = post_bar.data() + x * Q;
         bool any = false;
         for (int q = 0; q < Q; ++q) any |= g[q] != 0.0;
-        double ab = 0;
+        double ab = 0, tb = 0;
         if (any) {
-            collide_cell_vjp(o, before + x * Q, alpha[x], g, fb, ab);
+            collide_cell_vjp(o, before + x * Q, alpha[x], g, fb, ab, tau_at(o, x), tb);
         } else {
             for (int q = 0; q < Q; ++q) fb[q] = 0.0;
         }
         if (o.solid[x])
             for (int q = 0; q < Q; ++q) fb[q] += refl[x * Q + q];
         if (alpha_bar) alpha_bar[x] = ab;
+        if (tau_bar) tau_bar[x] = o.solid[x] ? 0.0 : tb;
     }
 }
 
@@ -1329,6 +1341,21 @@ void orc_interval_vjp(const orc_problem* o, const double* before, const double* 
     interval_vjp(*o, before, alpha, after_bar, f_bar, alpha_bar);
 }
 
+void orc_interval_vjp_tau(const orc_problem* o, const double* before, const double* alpha,
+                          const double* after_bar, double* f_bar, double* alpha_bar, double* tau_bar) {
+    interval_vjp(*o, before, alpha, after_bar, f_bar, alpha_bar, tau_bar);
+}
+
+int orc_set_tau(orc_problem* o, const double* tau) {
+    if (!tau) {
+        o->tau_cell.clear();
+        return 0;
+    }
+    if (o->coll != LBM_BGK) return 1;
+    o->tau_cell.assign(tau, tau + o->N);
+    return 0;
+}
+
 void orc_set_time(const orc_problem* o, int64_t t_index) { set_port_time(*o, t_index); }
 
 // Fixed-wall momentum-exchange loads (wall_exchange.rs: layout :44-70, loads
@@ -1357,7 +1384,7 @@ int64_t orc_wall_loads(const orc_problem* o, const double* before, const double*
             if (k >= 0 && L.c[q][o->ports[k].axis] == o->ports[k].sign) continue;
             if (forces) {
                 if (!collided) {
-                    collide_bgk(*o, before + x * Q, alpha[x], post.data());
+                    collide_bgk(*o, before + x * Q, alpha[x], post.data(), tau_at(*o, x));
                     collided = true;
                 }
                 const double mag = post[L.opp[q]] - L.w[q] + L.w[q] * datum_pa / unit;

@@ -79,6 +79,14 @@ void orc_vector_vjp(const orc_problem* o, const double* phi, const double* alpha
 void orc_interval_vjp(const orc_problem* o, const double* before, const double* alpha,
                       const double* after_bar, double* f_bar, double* alpha_bar);
 
+/* Tau::PerCell (solver.rs:171-187): per-cell relaxation times of the BGK
+ * collision (N values; NULL = the problem's uniform tau).  Returns 1 when
+ * the collision is not BGK.  orc_interval_vjp_tau also returns the
+ * per-cell tau cotangent of interval_vjp (tau_bar, solver.rs:642-674). */
+int orc_set_tau(orc_problem* o, const double* tau);
+void orc_interval_vjp_tau(const orc_problem* o, const double* before, const double* alpha,
+                          const double* after_bar, double* f_bar, double* alpha_bar, double* tau_bar);
+
 /* provider.rs:332-365 chain.  mode 0: fixed horizon with scan Every(K)
  * checkpoints (K <= 0: all states kept); mode 1: steady Neumann series at the
  * final state until |lambda_k| <= tol |lambda_0| or max_iter; mode 2: the

@@ -82,6 +82,10 @@ def lib() -> C.CDLL:
         L.orc_gradient.argtypes = [h, _dp, _dp, C.c_int64, C.c_int, C.c_int64, C.c_double, C.c_int64, _dp, _dp,
                                    C.POINTER(GradReport)]
         L.orc_mrt_basis.argtypes = [C.c_int, _dp, _dp, C.POINTER(C.c_int32)]
+        L.orc_set_tau.argtypes = [h, _dp]
+        L.orc_set_tau.restype = C.c_int
+        L.orc_interval_vjp_tau.argtypes = [h, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.orc_interval_vjp_tau.restype = None
         L.orc_set_time.argtypes = [h, C.c_int64]
         L.orc_set_time.restype = None
         L.orc_wall_loads.argtypes = [h, _dp, _dp, C.c_double, _dp]
@@ -228,6 +232,21 @@ class Oracle:
         out = np.empty((n, 3))
         lib().orc_wall_loads(self.h, _p(b), _p(al), float(pressure_datum_pa), _p(out))
         return out
+
+    def set_tau(self, tau):
+        """Per-cell relaxation times of the BGK collision (None: uniform)."""
+        self._tau = None if tau is None else np.ascontiguousarray(tau, dtype=np.float64).reshape(-1)
+        if lib().orc_set_tau(self.h, _p(self._tau)) != 0:
+            raise RuntimeError("per-cell tau needs the BGK collision")
+
+    def interval_vjp_tau(self, before, alpha, after_bar):
+        b = np.ascontiguousarray(before, dtype=np.float64).reshape(-1)
+        ab_ = np.ascontiguousarray(after_bar, dtype=np.float64).reshape(-1)
+        fb = np.empty_like(b)
+        abar, tbar = np.empty(self.cells), np.empty(self.cells)
+        lib().orc_interval_vjp_tau(self.h, _p(b), _p(np.ascontiguousarray(alpha, dtype=np.float64)), _p(ab_),
+                                   _p(fb), _p(abar), _p(tbar))
+        return fb.reshape(self.cells, self.q), abar, tbar
 
     def set_time(self, t_index: int):
         """Port values of the reconstruction producing state t_index."""
