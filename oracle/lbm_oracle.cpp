@@ -1358,6 +1358,98 @@ int orc_set_tau(orc_problem* o, const double* tau) {
 
 void orc_set_time(const orc_problem* o, int64_t t_index) { set_port_time(*o, t_index); }
 
+// ---------------------------------------------------------------- cell ranges
+// The pieces of interval (solver.rs:604-614) and interval_vjp (:642-674)
+// restricted to the cells [c0, c1), for x-slab domain decomposition checks:
+// each call reads only the slots the restricted computation needs, so
+// arrays that hold NaN outside a slab and its exchanged halo show every slot
+// the decomposition fails to provide.
+void orc_collide_range(const orc_problem* o, const double* before, const double* alpha, double* post, int64_t c0,
+                       int64_t c1) {
+    const int Q = o->Q;
+#pragma omp parallel for schedule(static)
+    for (int64_t x = c0; x < c1; ++x) collide_cell(*o, before + x * Q, alpha[x], post + x * Q, tau_at(*o, x));
+}
+
+void orc_stream_range(const orc_problem* o, const double* post, const double* before, double* after, int64_t c0,
+                      int64_t c1) {
+    const int Q = o->Q;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = c0 * Q; i < c1 * Q; ++i) {
+        const uint32_t s = o->source[i];
+        after[i] = s == NONE ? before[i] : post[s];
+    }
+}
+
+double orc_ports_range(const orc_problem* o, double* after, int64_t c0, int64_t c1) {
+    const int Q = o->Q;
+    double exch = 0;
+    for (const Port& p : o->ports)
+        for (int64_t cell : p.cells) {
+            if (cell < c0 || cell >= c1) continue;
+            double vals[27];
+            reconstruct(*o, p, after + cell * Q, vals);
+            for (int q = 0; q < Q; ++q) {
+                exch += vals[q] - after[cell * Q + q];
+                after[cell * Q + q] = vals[q];
+            }
+        }
+    return exch;
+}
+
+// refl = apply_ports_vjp of after_bar on the cells [c0, c1)
+void orc_ports_vjp_range(const orc_problem* o, const double* after_bar, double* refl, int64_t c0, int64_t c1) {
+    const int Q = o->Q;
+    for (int64_t i = c0 * Q; i < c1 * Q; ++i) refl[i] = after_bar[i];
+    for (const Port& p : o->ports)
+        for (int64_t cell : p.cells)
+            if (cell >= c0 && cell < c1)
+                for (int q = 0; q < Q; ++q) refl[cell * Q + q] = 0.0;
+    for (const Port& p : o->ports)
+        for (int64_t cell : p.cells) {
+            if (cell < c0 || cell >= c1) continue;
+            const double* g = after_bar + cell * Q;
+            for (int r = 0; r < Q; ++r) {
+                if (g[r] == 0.0) continue;
+                for (int k = 0; k < Q; ++k) refl[cell * Q + k] += p.jac[r * Q + k] * g[r];
+            }
+        }
+}
+
+// post_bar of the slots of the cells [c0, c1): Streaming::stream_vjp (solver.rs:138-157)
+void orc_stream_vjp_range(const orc_problem* o, const double* refl, double* post_bar, int64_t c0, int64_t c1) {
+    const int Q = o->Q;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = c0 * Q; i < c1 * Q; ++i) {
+        double acc = 0;
+        const uint32_t r0 = o->readers[2 * i], r1 = o->readers[2 * i + 1];
+        if (r0 != NONE) acc += refl[r0];
+        if (r1 != NONE) acc += refl[r1];
+        post_bar[i] = acc;
+    }
+}
+
+// f_bar and alpha_bar of the cells [c0, c1) from post_bar (collide_vjp) plus the
+// pass-through of solid cells' own slots (previous_bar)
+void orc_collide_vjp_range(const orc_problem* o, const double* before, const double* alpha, const double* post_bar,
+                           const double* refl, double* f_bar, double* alpha_bar, int64_t c0, int64_t c1) {
+    const int Q = o->Q;
+#pragma omp parallel for schedule(static)
+    for (int64_t x = c0; x < c1; ++x) {
+        double* fb = f_bar + x * Q;
+        const double* g = post_bar + x * Q;
+        bool any = false;
+        for (int q = 0; q < Q; ++q) any |= g[q] != 0.0;
+        double ab = 0, tb = 0;
+        if (any) collide_cell_vjp(*o, before + x * Q, alpha[x], g, fb, ab, tau_at(*o, x), tb);
+        else
+            for (int q = 0; q < Q; ++q) fb[q] = 0.0;
+        if (o->solid[x])
+            for (int q = 0; q < Q; ++q) fb[q] += refl[x * Q + q];
+        alpha_bar[x] = ab;
+    }
+}
+
 // Fixed-wall momentum-exchange loads (wall_exchange.rs: layout :44-70, loads
 // :79-84, loads_from_post :86-100): `before` is collided with the Guo-BGK
 // collision; for every blocked pull link q of a fluid cell (cells, then

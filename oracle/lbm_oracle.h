@@ -111,6 +111,22 @@ int orc_mrt_basis(int q, double* rows, double* norms, int32_t* groups);
  * producing state t_index; orc_interval / orc_interval_vjp then use them. */
 void orc_set_time(const orc_problem* o, int64_t t_index);
 
+/* interval / interval_vjp split into their pieces and restricted to the
+ * cells [c0, c1) (x-slab decomposition checks): collide, stream (pull through
+ * the source table), ports (returns the exchanged density of the range);
+ * apply_ports_vjp, stream_vjp (through the readers table) and the collision
+ * VJP with the solid pass-through.  Full-size arrays; only the slots each
+ * piece needs are read. */
+void orc_collide_range(const orc_problem* o, const double* before, const double* alpha, double* post, int64_t c0,
+                       int64_t c1);
+void orc_stream_range(const orc_problem* o, const double* post, const double* before, double* after, int64_t c0,
+                      int64_t c1);
+double orc_ports_range(const orc_problem* o, double* after, int64_t c0, int64_t c1);
+void orc_ports_vjp_range(const orc_problem* o, const double* after_bar, double* refl, int64_t c0, int64_t c1);
+void orc_stream_vjp_range(const orc_problem* o, const double* refl, double* post_bar, int64_t c0, int64_t c1);
+void orc_collide_vjp_range(const orc_problem* o, const double* before, const double* alpha, const double* post_bar,
+                           const double* refl, double* f_bar, double* alpha_bar, int64_t c0, int64_t c1);
+
 /* Port reconstruction of one cell (ports.rs:343-406) for port index k. */
 void orc_port_apply(const orc_problem* o, int port, const double* f_in, double* f_out);
 

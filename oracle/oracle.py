@@ -86,6 +86,19 @@ def lib() -> C.CDLL:
         L.orc_set_tau.restype = C.c_int
         L.orc_interval_vjp_tau.argtypes = [h, _dp, _dp, _dp, _dp, _dp, _dp]
         L.orc_interval_vjp_tau.restype = None
+        i64 = C.c_int64
+        L.orc_collide_range.argtypes = [h, _dp, _dp, _dp, i64, i64]
+        L.orc_collide_range.restype = None
+        L.orc_stream_range.argtypes = [h, _dp, _dp, _dp, i64, i64]
+        L.orc_stream_range.restype = None
+        L.orc_ports_range.argtypes = [h, _dp, i64, i64]
+        L.orc_ports_range.restype = C.c_double
+        L.orc_ports_vjp_range.argtypes = [h, _dp, _dp, i64, i64]
+        L.orc_ports_vjp_range.restype = None
+        L.orc_stream_vjp_range.argtypes = [h, _dp, _dp, i64, i64]
+        L.orc_stream_vjp_range.restype = None
+        L.orc_collide_vjp_range.argtypes = [h, _dp, _dp, _dp, _dp, _dp, _dp, i64, i64]
+        L.orc_collide_vjp_range.restype = None
         L.orc_set_time.argtypes = [h, C.c_int64]
         L.orc_set_time.restype = None
         L.orc_wall_loads.argtypes = [h, _dp, _dp, C.c_double, _dp]
