@@ -9,7 +9,7 @@ import ctypes as C
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "liblbm_b200.so"
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 # status codes
 LBM_OK, LBM_E_CONTRACT, LBM_E_CONVERGENCE, LBM_E_CUDA, LBM_E_STATE = 0, 1, 2, 3, 4
@@ -50,6 +50,16 @@ EXPORTS = [
     "lbm_step_vjp_tau",
     "lbm_set_tau",
     "lbm_design_vjp",
+    "lbm_create_slab",
+    "lbm_slab_begin",
+    "lbm_slab_step",
+    "lbm_slab_inspect",
+    "lbm_halo_bytes",
+    "lbm_halo_pack",
+    "lbm_halo_unpack",
+    "lbm_slab_adjoint_begin",
+    "lbm_slab_adjoint_step",
+    "lbm_slab_gradient",
     "lbm_state_stats_noalloc",
 ]
 
@@ -133,6 +143,16 @@ class AdjointOpts(C.Structure):
     ]
 
 
+class SlabDiag(C.Structure):
+    _fields_ = [
+        ("mass", C.c_double),
+        ("exchange", C.c_double),
+        ("minimum_population", C.c_double),
+        ("maximum_speed2", C.c_double),
+        ("nonfinite", C.c_int32),
+    ]
+
+
 class AdjointReport(C.Structure):
     _fields_ = [
         ("residual", C.c_double),
@@ -186,6 +206,16 @@ def _declare(lib: C.CDLL) -> None:
     lib.lbm_fields.argtypes = [h, _dp, _dp, _dp]
     lib.lbm_gradient.argtypes = [h, _dp, C.POINTER(AdjointOpts), _dp, C.POINTER(AdjointReport)]
     lib.lbm_step_vjp.argtypes = [h, _dp, _dp, _dp, _dp, C.c_size_t]
+    lib.lbm_create_slab.argtypes = [C.POINTER(Problem), C.c_int32, C.c_int32, C.c_int32, C.POINTER(h)]
+    lib.lbm_slab_begin.argtypes = [h]
+    lib.lbm_slab_step.argtypes = [h, C.POINTER(SlabDiag)]
+    lib.lbm_slab_inspect.argtypes = [h, C.POINTER(SlabDiag)]
+    lib.lbm_halo_bytes.argtypes = [h, C.c_int32, C.POINTER(C.c_size_t)]
+    lib.lbm_halo_pack.argtypes = [h, C.c_int32, C.c_int32, C.c_void_p]
+    lib.lbm_halo_unpack.argtypes = [h, C.c_int32, C.c_int32, C.c_void_p]
+    lib.lbm_slab_adjoint_begin.argtypes = [h, _dp, _dp]
+    lib.lbm_slab_adjoint_step.argtypes = [h, _dp]
+    lib.lbm_slab_gradient.argtypes = [h, _dp, C.c_size_t]
     lib.lbm_step_vjp_tau.argtypes = [h, _dp, _dp, _dp, _dp, _dp, C.c_size_t]
     lib.lbm_set_tau.argtypes = [h, _dp, C.c_size_t]
     lib.lbm_design_vjp.argtypes = [h, _dp, _dp, C.c_size_t]

@@ -108,6 +108,7 @@ struct ObjArgs {
     double* norm2;
     int32_t write_lambda;
     int32_t port_transpose;
+    uint32_t c_begin, c_end;  // cells taken into account (an x-slab's owned range; 0, n otherwise)
 };
 
 struct DesignArgs {
@@ -164,6 +165,10 @@ cudaError_t launch_wall_loads(int Q, int storage, const Geometry& G, const Physi
 cudaError_t launch_tau_bar(int Q, const Geometry& G, const Physics& P, const float* g, const float* lam,
                            const uint32_t* mask, const float* alpha, const float* omega_cell, double* out, int grid,
                            cudaStream_t s);
+// Slab halos: directions `dirs` of the x plane starting at cell plane0 (sx
+// cells) of a stored array (storage type) to (unpack = 0) or from (1) buf.
+cudaError_t launch_halo_copy(int storage, void* arr, int64_t n, int64_t plane0, int64_t sx, const int32_t* dirs,
+                             int ndir, void* buf, int unpack, cudaStream_t s);
 cudaError_t launch_canon_lam(int Q, int lstorage, const Geometry& G, const void* lam, const uint32_t* mask,
                              float inv_scale, float* out, int grid, cudaStream_t s);
 cudaError_t launch_seed_lam(int Q, int lstorage, const Geometry& G, void* lam, const uint32_t* mask,

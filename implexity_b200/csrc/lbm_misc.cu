@@ -43,6 +43,7 @@ __global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
     acc.init();
     double nsum = 0.0;
     for (uint32_t x = blockIdx.x * BLOCK + threadIdx.x; x < (uint32_t)n; x += gridDim.x * BLOCK) {
+        if (x < a.c_begin || x >= a.c_end) continue;  // ghost planes of an x-slab belong to other ranks
         const uint32_t m = a.mask[x];
         if (m & MASK_SOLID) {
             if constexpr (MODE == 0) acc.add(5, (double)a.phi[x]);
@@ -318,6 +319,26 @@ __global__ void __launch_bounds__(BLOCK) k_tau_bar(Geometry G, Physics P, const 
     }
 }
 
+// ------------------------------------------------------------------ slab halos
+// x-slab decomposition: the face-crossing directions of one x plane of a
+// stored array (state or adjoint) to or from a contiguous buffer laid out
+// [direction][cell of the plane].  Plain coalesced copies.
+struct HaloDirs {
+    int32_t q[9];
+    int32_t n;
+};
+template <typename T>
+__global__ void __launch_bounds__(BLOCK) k_halo_copy(T* arr, uint32_t n, uint32_t plane0, uint32_t sx, HaloDirs d,
+                                                     T* buf, int unpack) {
+    const uint32_t total = sx * (uint32_t)d.n;
+    for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < total; i += gridDim.x * BLOCK) {
+        const uint32_t k = i / sx, j = i - k * sx;
+        T* slot = arr + (size_t)d.q[k] * n + plane0 + j;
+        if (unpack) *slot = buf[i];
+        else buf[i] = *slot;
+    }
+}
+
 // ------------------------------------------------------------------ bounded-wait probe
 // One thread waits on an mbarrier that nothing arrives at, with the stepping
 // kernels' bounded wait and a short limit: the wait must give up, set the
@@ -527,6 +548,19 @@ cudaError_t launch_tau_bar(int Q, const Geometry& G, const Physics& P, const flo
                            cudaStream_t s) {
     if (Q == 19) k_tau_bar<19><<<grid, BLOCK, 0, s>>>(G, P, g, lam, mask, alpha, omega_cell, out);
     else k_tau_bar<27><<<grid, BLOCK, 0, s>>>(G, P, g, lam, mask, alpha, omega_cell, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_halo_copy(int storage, void* arr, int64_t n, int64_t plane0, int64_t sx, const int32_t* dirs,
+                             int ndir, void* buf, int unpack, cudaStream_t s) {
+    if (ndir < 1 || ndir > 9) return cudaErrorInvalidValue;
+    HaloDirs d{};
+    for (int k = 0; k < ndir; ++k) d.q[k] = dirs[k];
+    d.n = ndir;
+    const int grid = (int)std::min<int64_t>((sx * ndir + BLOCK - 1) / BLOCK, 1024);
+    LBM_STORAGE_DISPATCH(storage, T,
+                         k_halo_copy<T><<<grid, BLOCK, 0, s>>>(static_cast<T*>(arr), (uint32_t)n, (uint32_t)plane0,
+                                                               (uint32_t)sx, d, static_cast<T*>(buf), unpack))
     return cudaGetLastError();
 }
 

@@ -318,6 +318,10 @@ struct Checkpoint {
     bool pending;
 };
 
+namespace {
+struct AdjState;
+}  // namespace
+
 struct lbm_handle {
     // --- normalised problem
     int Q = 19, coll = LBM_BGK, storage = LBM_STORE_F32;
@@ -344,6 +348,7 @@ struct lbm_handle {
     DevBuf pop, mask, alpha, phi, raw, den, slope, cls_d, fixed_d, offsets_d, ports_d, partial, counter, diag;
     DevBuf lam, record, abar, abar_final, phibar, scale, grad, norm2, sums, scratch, errflag;
     DevBuf omega_cell, tau_state, tau_bar;
+    AdjState* slab_adj = nullptr;  // x-slab steady adjoint in progress (lbm_slab_adjoint_begin)
     int lam_storage = LBM_STORE_F32;
     // --- ports: normalised specs with their signals; pulsatile ports keep one
     // set of maps per state index on the device (ensure_port_maps)
@@ -372,6 +377,12 @@ struct lbm_handle {
     // a non-finite population was loaded into a solid cell (lbm_set_populations):
     // solid cells are never stepped, so every later state carries it too
     bool solid_nonfinite = false;
+    // x-slab of a larger problem (lbm_create_slab): the owned planes are
+    // [slab_hl, slab_hl + slab_own) of the local grid, the others ghost planes;
+    // responses, seeds and port pressure weights use the whole problem's counts
+    bool slab = false;
+    int32_t slab_hl = 0, slab_hr = 0, slab_own = 0;
+    int64_t global_fluid = -1, global_inlet = -1, global_outlet = -1;
     int64_t t = 0;
     std::string err;
 
@@ -410,6 +421,12 @@ void require(bool ok, const char* msg) {
 }
 bool finite_positive(double v) { return std::isfinite(v) && v > 0; }
 
+// Counts that scale the responses: the whole problem's for an x-slab.
+int64_t resp_fluid(const lbm_handle& h) { return h.global_fluid >= 0 ? h.global_fluid : h.fluid_cells; }
+bool resp_both_ports(const lbm_handle& h) {
+    return (h.global_inlet >= 0 ? h.global_inlet : h.n_inlet) > 0 && (h.global_outlet >= 0 ? h.global_outlet : h.n_outlet) > 0;
+}
+
 // The affine port maps (shifted variables) of every port for the values in
 // force at time t seconds: bias and Jacobian of the FP64 reconstruction over
 // the unknown populations, tabulated at the weights.
@@ -434,8 +451,9 @@ std::vector<PortMap> port_maps_at(const lbm_handle& h, double t_s) {
             for (int r = 0; r < Q; ++r)
                 if (M.unknown_mask & (1u << r)) M.jac[r][kq] = (float)(r1[r] - r0[r]);
         }
-        const bool both = h.n_inlet > 0 && h.n_outlet > 0;
-        M.dp_weight = !both ? 0.f : spec.pressure ? (float)(-1.0 / h.n_outlet) : (float)(1.0 / h.n_inlet);
+        const int64_t ni = h.global_inlet >= 0 ? h.global_inlet : h.n_inlet;
+        const int64_t no = h.global_outlet >= 0 ? h.global_outlet : h.n_outlet;
+        M.dp_weight = !resp_both_ports(h) ? 0.f : spec.pressure ? (float)(-1.0 / no) : (float)(1.0 / ni);
     }
     return maps;
 }
@@ -1026,6 +1044,9 @@ ObjArgs obj_args(lbm_handle& h) {
     a.dens = (float)h.density;
     a.dt_s = (float)h.dt;
     a.red = reduce_of(h);
+    const int64_t sxo = h.G.sx;
+    a.c_begin = h.slab ? (uint32_t)(h.slab_hl * sxo) : 0u;
+    a.c_end = h.slab ? (uint32_t)((h.slab_hl + h.slab_own) * sxo) : (uint32_t)h.n();
     return a;
 }
 
@@ -1035,14 +1056,14 @@ double visc_scale(const lbm_handle& h) { return h.density * std::pow(h.dx, 5) / 
 void sums_to_responses(const lbm_handle& h, const double* s, double* out8) {
     double v[8];
     for (int k = 0; k < 8; ++k) v[k] = s[2 * k] + s[2 * k + 1];
-    const double nf = (double)h.fluid_cells, dv = h.dx * h.dx * h.dx;
+    const double nf = (double)resp_fluid(h), dv = h.dx * h.dx * h.dx;
     out8[0] = v[0] / nf;
     out8[1] = v[1] / nf;
     out8[2] = v[2] / nf;
     out8[3] = 0.5 * v[3] * dv;
     out8[4] = v[4] * dv;
     out8[5] = v[5] * dv;
-    out8[6] = (h.n_inlet > 0 && h.n_outlet > 0) ? v[6] : 0.0;
+    out8[6] = resp_both_ports(h) ? v[6] : 0.0;
     out8[7] = v[7] * visc_scale(h);
 }
 
@@ -1172,14 +1193,14 @@ double read_norm(lbm_handle& h) {
 // `scale` (1/T for a state of a time average: the fluid volume does not
 // change in time, so its mean is itself).
 void response_weights(const lbm_handle& h, const double* w, double scale, double* out8) {
-    const double nf = (double)h.fluid_cells, dv = h.dx * h.dx * h.dx;
+    const double nf = (double)resp_fluid(h), dv = h.dx * h.dx * h.dx;
     out8[0] = scale * w[0] / nf;
     out8[1] = scale * w[1] / nf;
     out8[2] = scale * w[2] / nf;
     out8[3] = scale * 0.5 * w[3] * dv;
     out8[4] = scale * w[4] * dv;
     out8[5] = w[5] * dv;
-    out8[6] = (h.n_inlet > 0 && h.n_outlet > 0) ? scale * w[6] : 0.0;
+    out8[6] = resp_both_ports(h) ? scale * w[6] : 0.0;
     out8[7] = scale * w[7] * visc_scale(h);
 }
 
@@ -1751,6 +1772,8 @@ lbm_status lbm_create(const lbm_problem_t* problem, lbm_handle** out) {
 
 void lbm_destroy(lbm_handle* h) {
     if (!h) return;
+    delete h->slab_adj;
+    h->slab_adj = nullptr;
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->ckpts.clear();
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -1864,6 +1887,12 @@ lbm_status lbm_set_populations(lbm_handle* h, const double* f, size_t n) {
         check_n(*h, n, (size_t)(N * Q), "populations");
         std::vector<float> g((size_t)N * Q);
         bool solid_nonfinite = false;
+    // x-slab of a larger problem (lbm_create_slab): the owned planes are
+    // [slab_hl, slab_hl + slab_own) of the local grid, the others ghost planes;
+    // responses, seeds and port pressure weights use the whole problem's counts
+    bool slab = false;
+    int32_t slab_hl = 0, slab_hr = 0, slab_own = 0;
+    int64_t global_fluid = -1, global_inlet = -1, global_outlet = -1;
         for (int64_t x = 0; x < N; ++x) {
             for (int q = 0; q < Q; ++q) g[(size_t)q * N + x] = (float)(f[x * Q + q] - h->L.w[q]);
             if (h->cls[x] == 0)  // solid
@@ -2167,6 +2196,279 @@ lbm_status lbm_step_vjp_tau(lbm_handle* h, const double* state, const double* la
             throw ContractError("per-cell relaxation times need the BGK collision (Tau::PerCell of the density-design "
                                 "solver)");
         return step_vjp_impl(h, state, lambda_next, lambda, alpha_bar, tau_bar, n_populations);
+    });
+}
+
+// ------------------------------------------------------------ x-slab decomposition
+lbm_status lbm_create_slab(const lbm_problem_t* problem, int32_t x_begin, int32_t x_end, int32_t halo,
+                           lbm_handle** out) {
+    if (!out) return LBM_E_CONTRACT;
+    *out = nullptr;
+    try {
+        if (!problem) throw ContractError("problem must not be NULL");
+        const lbm_problem_t& P = *problem;
+        const int nx = P.shape[0], ny = P.shape[1], nz = P.shape[2];
+        require(nx >= 2 && ny >= 2 && nz >= 2, "LBM shape must contain three integers >= 2");
+        require(P.solid_mask && P.design_region && P.fixed_design, "solid_mask must be a shape-matched boolean array");
+        require(x_begin >= 0 && x_end <= nx && x_end - x_begin >= 2,
+                "x-slab: the owned planes [x_begin, x_end) must lie in the grid and number two at least");
+        require(!P.time_average, "x-slab decomposition does not run the time-averaged objective");
+        const bool per = P.periodic_axes[0] != 0;
+        int reach = 0;
+        if (P.filter_kind == LBM_FILTER_BOX) reach = P.box_half_width;
+        else if (P.filter_radius_m > 0 && P.spacing_m > 0) reach = (int)std::ceil(P.filter_radius_m / P.spacing_m);
+        require(halo >= 1 && halo >= reach, "x-slab: halo must be at least 1 and cover the design filter's reach");
+        const int hl = per ? halo : std::min(halo, (int)x_begin);
+        const int hr = per ? halo : std::min(halo, nx - (int)x_end);
+        const int own = x_end - x_begin, nxl = hl + own + hr;
+        require(!per || nxl <= nx, "x-slab: the slab and its ghost planes must not wrap onto themselves");
+        const int64_t sx = (int64_t)ny * nz, nl = (int64_t)nxl * sx, ng = (int64_t)nx * sx;
+        auto gplane = [&](int pl) { return (int64_t)(((x_begin - hl + pl) % nx + nx) % nx); };
+        std::vector<uint8_t> solid(nl), design(nl);
+        std::vector<double> fixed(nl);
+        for (int pl = 0; pl < nxl; ++pl)
+            for (int64_t j = 0; j < sx; ++j) {
+                const int64_t g = gplane(pl) * sx + j, l = (int64_t)pl * sx + j;
+                solid[l] = P.solid_mask[g] ? 1 : 0;
+                design[l] = P.design_region[g] ? 1 : 0;
+                fixed[l] = P.fixed_design[g];
+            }
+        // ports: on the x faces only (their cells then lie in one slab); the
+        // pressure-drop weights keep the whole problem's port cell counts
+        std::vector<lbm_port_t> ports;
+        std::vector<std::vector<uint8_t>> pmask;
+        int64_t gin = 0, gout = 0;
+        for (int k = 0; k < P.n_ports; ++k) {
+            const lbm_port_t& pt = P.ports[k];
+            require(pt.mask != nullptr, "Port mask must be a shape-matched boolean array");
+            require(pt.face == LBM_XMIN || pt.face == LBM_XMAX, "x-slab decomposition supports ports on the x faces only");
+            int64_t cnt = 0;
+            for (int64_t x = 0; x < ng; ++x) cnt += pt.mask[x] ? 1 : 0;
+            (pt.kind == LBM_PORT_PRESSURE ? gout : gin) += cnt;
+            std::vector<uint8_t> m(nl, 0);
+            bool any = false;
+            for (int pl = hl; pl < hl + own; ++pl)
+                for (int64_t j = 0; j < sx; ++j) {
+                    const uint8_t v = pt.mask[gplane(pl) * sx + j] ? 1 : 0;
+                    m[(int64_t)pl * sx + j] = v;
+                    any = any || v;
+                }
+            if (any) {
+                pmask.push_back(std::move(m));
+                ports.push_back(pt);
+            }
+        }
+        for (size_t k = 0; k < ports.size(); ++k) ports[k].mask = pmask[k].data();
+        int64_t gf = 0;
+        for (int64_t x = 0; x < ng; ++x) gf += P.solid_mask[x] ? 0 : 1;
+        lbm_problem_t L = P;
+        L.shape[0] = nxl;
+        L.periodic_axes[0] = 0;
+        L.solid_mask = solid.data();
+        L.design_region = design.data();
+        L.fixed_design = fixed.data();
+        L.n_ports = (int32_t)ports.size();
+        L.ports = ports.empty() ? nullptr : ports.data();
+        auto h = std::make_unique<lbm_handle>();
+        h->slab = true;
+        h->slab_hl = hl;
+        h->slab_hr = hr;
+        h->slab_own = own;
+        h->global_fluid = gf;
+        h->global_inlet = gin;
+        h->global_outlet = gout;
+        validate_and_build(*h, L);
+        // ghost planes hold exchanged values and are never stepped
+        std::vector<uint32_t> mask((size_t)nl);
+        CK(cudaMemcpy(mask.data(), h->mask.p, (size_t)nl * 4, cudaMemcpyDeviceToHost));
+        int64_t fluid_own = 0;
+        for (int64_t x = 0; x < nl; ++x) {
+            const int64_t pl = x / sx;
+            if (pl < hl || pl >= hl + own) mask[x] |= MASK_SOLID;
+            else fluid_own += solid[x] ? 0 : 1;
+        }
+        CK(cudaMemcpy(h->mask.p, mask.data(), (size_t)nl * 4, cudaMemcpyHostToDevice));
+        h->fluid_cells = fluid_own;
+        g_create_error.clear();
+        *out = h.release();
+        return LBM_OK;
+    } catch (const ContractError& e) {
+        g_create_error = e.what();
+        return LBM_E_CONTRACT;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        return LBM_E_CUDA;
+    }
+}
+
+namespace {
+void require_slab(const lbm_handle& h) {
+    if (!h.slab) throw StateError("not an x-slab handle (lbm_create_slab)");
+}
+
+// Directions of a halo message: the state sends c_x = +1 to the right and
+// -1 to the left, the adjoint the mirrored sets.
+int halo_dirs(const lbm_handle& h, int kind, int side, int32_t* dirs) {
+    const int sign = ((kind == 0) == (side == 1)) ? 1 : -1;
+    int nd = 0;
+    for (int q = 0; q < h.Q; ++q)
+        if (h.L.c[q][0] == sign) dirs[nd++] = q;
+    return nd;
+}
+
+void read_slab_diag(lbm_handle& h, lbm_slab_diag_t* out) {
+    StepDiag d{};
+    CK(cudaMemcpyAsync(&d, h.diag.p, sizeof(d), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    check_errflag(h);
+    if (out) {
+        out->mass = (double)h.fluid_cells + d.mass_hi + d.mass_lo;
+        out->exchange = d.exch_hi + d.exch_lo;
+        out->minimum_population = d.min_f;
+        out->maximum_speed2 = d.max_u2;
+        out->nonfinite = d.nonfinite;
+    }
+}
+}  // namespace
+
+lbm_status lbm_slab_begin(lbm_handle* h) {
+    return guarded(h, [&]() {
+        require_slab(*h);
+        require_design(*h);
+        init_state(*h);
+        h->forward_done = false;
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_slab_step(lbm_handle* h, lbm_slab_diag_t* diag) {
+    return guarded(h, [&]() {
+        require_slab(*h);
+        if (!h->state_valid) throw StateError("no current state: call lbm_slab_begin first");
+        h->diag.alloc(sizeof(StepDiag), &h->device_bytes);
+        step(*h, h->diag.as<StepDiag>(), nullptr);
+        read_slab_diag(*h, diag);
+        h->forward_done = false;
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_slab_inspect(lbm_handle* h, lbm_slab_diag_t* diag) {
+    return guarded(h, [&]() {
+        require_slab(*h);
+        if (!h->state_valid) throw StateError("no current state: call lbm_slab_begin first");
+        h->diag.alloc(sizeof(StepDiag), &h->device_bytes);
+        inspect(*h, h->diag.as<StepDiag>(), nullptr);
+        read_slab_diag(*h, diag);
+        h->forward_done = true;
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_halo_bytes(const lbm_handle* h, int32_t kind, size_t* bytes) {
+    if (!h || !bytes || (kind != 0 && kind != 1)) return LBM_E_CONTRACT;
+    int32_t dirs[27];
+    const int nd = halo_dirs(*h, kind, 1, dirs);
+    const int st = kind == 0 ? h->storage : LBM_STORE_F32;
+    *bytes = (size_t)nd * (size_t)h->G.sx * storage_bytes(st);
+    return LBM_OK;
+}
+
+namespace {
+lbm_status halo_move(lbm_handle* h, int32_t kind, int32_t side, void* buf, int unpack) {
+    return guarded(h, [&]() {
+        require_slab(*h);
+        if ((kind != 0 && kind != 1) || (side != 0 && side != 1) || !buf)
+            throw ContractError("halo: kind must be 0 (state) or 1 (adjoint), side 0 (left) or 1 (right), buffer non-NULL");
+        if (side == 0 ? h->slab_hl < 1 : h->slab_hr < 1)
+            throw ContractError("halo: this slab has no neighbour on that side");
+        if (kind == 0 && !h->state_valid) throw StateError("halo: no current state");
+        if (kind == 1 && !h->slab_adj) throw StateError("halo: no adjoint in progress (lbm_slab_adjoint_begin)");
+        int32_t dirs[27];
+        // what arrives from a side is the neighbour's message travelling the other way
+        const int nd = halo_dirs(*h, kind, unpack ? 1 - side : side, dirs);
+        const int64_t sx = h->G.sx;
+        const int64_t plane = unpack ? (side == 0 ? h->slab_hl - 1 : h->slab_hl + h->slab_own)
+                                     : (side == 0 ? h->slab_hl : h->slab_hl + h->slab_own - 1);
+        void* arr = kind == 0 ? h->popA() : h->lamA();
+        const int st = kind == 0 ? h->storage : LBM_STORE_F32;
+        if (kind == 0 && h->restored) throw StateError("halo: the current state is a restored checkpoint");
+        CK(launch_halo_copy(st, arr, h->n(), plane * sx, sx, dirs, nd, buf, unpack, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return LBM_OK;
+    });
+}
+}  // namespace
+
+lbm_status lbm_halo_pack(lbm_handle* h, int32_t kind, int32_t side, void* device_buffer) {
+    return halo_move(h, kind, side, device_buffer, 0);
+}
+
+lbm_status lbm_halo_unpack(lbm_handle* h, int32_t kind, int32_t side, const void* device_buffer) {
+    return halo_move(h, kind, side, const_cast<void*>(device_buffer), 1);
+}
+
+lbm_status lbm_slab_adjoint_begin(lbm_handle* h, const double* weights, double* norm2) {
+    return guarded(h, [&]() {
+        require_slab(*h);
+        if (!h->forward_done) throw StateError("lbm_slab_inspect must follow the last step before the adjoint");
+        if (!weights) throw ContractError("weights must not be NULL");
+        alloc_adjoint(*h, LBM_STORE_F32);
+        int64_t* ctr = &h->device_bytes;
+        const int64_t n = h->n();
+        h->record.alloc(((size_t)n * 4 + CELL_PAD) * sizeof(float), ctr);
+        h->abar_final.alloc((size_t)n * 4, ctr);
+        h->phibar.alloc((size_t)n * 4, ctr);
+        delete h->slab_adj;
+        h->slab_adj = new AdjState();  // unit scale: the values cross ranks as they are
+        // cotangents of the ghost planes belong to other ranks
+        CK(cudaMemsetAsync(h->abar.p, 0, (size_t)n * 4, h->stream));
+        CK(cudaMemsetAsync(h->abar_final.p, 0, (size_t)n * 4, h->stream));
+        CK(cudaMemsetAsync(h->phibar.p, 0, (size_t)n * 4, h->stream));
+        ObjArgs a = obj_args(*h);
+        response_weights(*h, weights, 1.0, a.w);
+        a.lam = h->lamA();
+        a.abar_final = h->abar_final.as<float>();
+        a.phibar = h->phibar.as<float>();
+        a.record = h->record.as<float>();
+        a.port_transpose = 1;
+        a.norm2 = h->norm2.as<double>();
+        a.write_lambda = 1;
+        a.lam_scale = 1.f;
+        CK(launch_objective(h->Q, h->storage, LBM_STORE_F32, 1, a, grid_for(*h), h->stream));
+        double s2[2];
+        CK(cudaMemcpyAsync(s2, h->norm2.p, sizeof(s2), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (norm2) *norm2 = s2[0] + s2[1];
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_slab_adjoint_step(lbm_handle* h, double* norm2) {
+    return guarded(h, [&]() {
+        require_slab(*h);
+        if (!h->slab_adj) throw StateError("no adjoint in progress (lbm_slab_adjoint_begin)");
+        adjoint_step(*h, *h->slab_adj, h->record.as<float>(), norm2 != nullptr);
+        if (norm2) {
+            double s2[2];
+            CK(cudaMemcpyAsync(s2, h->norm2.p, sizeof(s2), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            *norm2 = s2[0] + s2[1];
+        }
+        return LBM_OK;
+    });
+}
+
+lbm_status lbm_slab_gradient(lbm_handle* h, double* grad, size_t n) {
+    return guarded(h, [&]() {
+        require_slab(*h);
+        if (!h->slab_adj) throw StateError("no adjoint in progress (lbm_slab_adjoint_begin)");
+        check_n(*h, n, (size_t)h->n(), "grad");
+        // the steps' alpha cotangents exist on owned fluid cells only; the
+        // other entries were cleared when the adjoint began
+        finish_gradient(*h, *h->slab_adj, h->slab_adj->steps > 0, grad);
+        check_errflag(*h);
+        return LBM_OK;
     });
 }
 

@@ -161,13 +161,14 @@ class SlabDriver:
       forward_begin()                 the initial state
       forward_stage(t)                work of step t before the exchange (may be none)
       forward_finish(t)               the rest of step t
+      exchange_before_end, forward_end()  (optional) a last exchange and a read of the final state
       diagnostics() -> (n_states, 5)  partial admission sums of every state: mass, exchange,
                                       min population, max |u|^2, non-finite flag
       responses() -> 8                partial responses of the final state
       adjoint_begin(weights) -> |lambda_0|^2 partial
       adjoint_stage()                 work of a transposed step before the exchange (may be none)
       adjoint_finish(want_norm) -> |lambda_k|^2 partial
-      gradient() -> (offset, values)  partial design gradient over a contiguous range of cells
+      gradient() -> array             this rank's share of the design gradient (whole-problem size)
     """
 
     def __init__(self, backend, comm, mach_limit: float, mass_drift_limit: float = 1e-6):
@@ -195,6 +196,11 @@ class SlabDriver:
             self.b.forward_stage(t)
             self._exchange("state")
             self.b.forward_finish(t)
+        if getattr(self.b, "exchange_before_end", False):
+            # a backend that reduces a state while reading it needs the last halos too
+            self._exchange("state")
+        if hasattr(self.b, "forward_end"):
+            self.b.forward_end()
         d = np.asarray(self.b.diagnostics(), dtype=np.float64)
         sums = self.c.allreduce(d[:, :2].ravel(), "sum").reshape(-1, 2)
         mins = self.c.allreduce(d[:, 2], "min")
@@ -227,8 +233,5 @@ class SlabDriver:
                 resid = float(np.sqrt(self.c.allreduce([nrm2], "sum")[0])) / n0
                 if resid <= tolerance:
                     break
-        off, part = self.b.gradient()
-        n = self.b.cells_global
-        g = np.zeros(n)
-        g[off:off + part.size] = part
-        return self.c.allreduce(g, "sum"), {"iterations": it, "residual": resid, "converged": resid <= tolerance}
+        return self.c.allreduce(self.b.gradient(), "sum"), {"iterations": it, "residual": resid,
+                                                          "converged": resid <= tolerance}

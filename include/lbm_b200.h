@@ -51,7 +51,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 4
+#define LBM_ABI_VERSION 5
 
 #if defined(__GNUC__)
 #define LBM_API __attribute__((visibility("default")))
@@ -393,6 +393,55 @@ LBM_API lbm_status lbm_step_vjp_tau(lbm_handle* h, const double* state, const do
 /* Design-map transpose alone (DesignMap::vjp, design.rs:219-243) for the
  * design last set: out[N] = d phi / d raw ^T phi_bar. */
 LBM_API lbm_status lbm_design_vjp(lbm_handle* h, const double* phi_bar, double* out, size_t n);
+
+/* ---- x-slab decomposition (several GPUs) ------------------------------- */
+
+/* The reference parallelises this path over cells in one process (rayon,
+ * solver.rs:131-136, moving/field.rs:570-611); here a problem is split along
+ * x over one handle per GPU.  lbm_create_slab creates the handle of the owned
+ * planes [x_begin, x_end) of `problem` (the whole problem's description)
+ * plus `halo` ghost planes on each side that has a neighbour (all sides when
+ * x is periodic; halo >= 1 and >= the design filter's reach).  The handle's
+ * grid is the slab with its ghost planes: lbm_set_design takes the raw design
+ * of those planes (in order, wrapping for periodic x), lbm_slab_gradient
+ * returns the gradient contributions over them, to be summed over ranks.
+ * Ports must lie on the x faces.  Responses (lbm_responses) are this rank's
+ * share, normalised with the whole problem's fluid and port cell counts:
+ * their sum over ranks is the problem's.  Not with time_average.
+ *
+ * One step of the driver: exchange the state halos (lbm_halo_pack of the
+ * current state on each side with a neighbour, transfer, lbm_halo_unpack
+ * of what arrived), then lbm_slab_step.  A state halo message carries the
+ * populations with c_x = +1 (right side) or -1 (left) of the boundary plane;
+ * an adjoint message the mirrored sets (lbm_halo_bytes gives the size; device
+ * buffers; kind 0 state, 1 adjoint; side 0 left, 1 right).  Each step returns
+ * this rank's admission sums of the state it read (mass sum(rho), port
+ * exchange, minimum population, maximum |u|^2, non-finite flag); after the
+ * last step an exchange and lbm_slab_inspect give the final state's.  The
+ * steady adjoint runs the same way: lbm_slab_adjoint_begin seeds it at the
+ * current state (FP32, unit scale), then per iteration an adjoint exchange and
+ * lbm_slab_adjoint_step (|lambda|^2 of this rank when norm2 is non-NULL),
+ * then lbm_slab_gradient.  The scalars are reduced over ranks by the caller
+ * (implexity_b200/slabs.py). */
+typedef struct {
+    double mass;
+    double exchange;
+    double minimum_population;
+    double maximum_speed2;
+    int32_t nonfinite;
+} lbm_slab_diag_t;
+
+LBM_API lbm_status lbm_create_slab(const lbm_problem_t* problem, int32_t x_begin, int32_t x_end, int32_t halo,
+                                   lbm_handle** out);
+LBM_API lbm_status lbm_slab_begin(lbm_handle* h);
+LBM_API lbm_status lbm_slab_step(lbm_handle* h, lbm_slab_diag_t* diag);
+LBM_API lbm_status lbm_slab_inspect(lbm_handle* h, lbm_slab_diag_t* diag);
+LBM_API lbm_status lbm_halo_bytes(const lbm_handle* h, int32_t kind, size_t* bytes);
+LBM_API lbm_status lbm_halo_pack(lbm_handle* h, int32_t kind, int32_t side, void* device_buffer);
+LBM_API lbm_status lbm_halo_unpack(lbm_handle* h, int32_t kind, int32_t side, const void* device_buffer);
+LBM_API lbm_status lbm_slab_adjoint_begin(lbm_handle* h, const double* weights, double* norm2);
+LBM_API lbm_status lbm_slab_adjoint_step(lbm_handle* h, double* norm2);
+LBM_API lbm_status lbm_slab_gradient(lbm_handle* h, double* grad, size_t n);
 
 /* ---- state statistics without device allocation ------------------------ */
 

@@ -151,4 +151,4 @@ class OracleSlab:
     def gradient(self):
         phibar = self.phibar + (self.abar + self.abar_final) * self.dres
         phibar = np.where(self.own, phibar, 0.0)
-        return 0, self.o.design_vjp(self.raw, phibar)
+        return self.o.design_vjp(self.raw, phibar)
