@@ -180,12 +180,16 @@ class SlabDriver:
         self.peers = {"left": s.left, "right": s.right}
 
     def _exchange(self, kind: str):
-        plan = halo_plan(self.b.q, kind)
+        full = halo_plan(self.b.q, kind)
+        plan = [m for m in full if self.peers[m.side] is not None]
+        if not plan:
+            return
         sends = {m.side: self.b.halo_pack(kind, m) for m in plan}
-        # a message leaving on one side arrives from the other side at the neighbour
-        arrived = self.c.exchange(sends, {"left": sends["right"], "right": sends["left"]}, self.peers)
+        # both messages of a plan have the same size (as many +x as -x directions)
+        like = next(iter(sends.values()))
+        arrived = self.c.exchange(sends, {"left": like, "right": like}, self.peers)
         mirror = {"left": "right", "right": "left"}
-        for m in plan:
+        for m in full:
             src = mirror[m.side]  # the neighbour on src sent its m.side message to us
             if src in arrived:
                 self.b.halo_unpack(kind, HaloMessage(src, m.directions), arrived[src])
