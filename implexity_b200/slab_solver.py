@@ -116,6 +116,10 @@ class SlabSolver:
         self._diag(self.lib.lbm_slab_step)
 
     exchange_before_end = True
+    # the initial state is written into the slots each cell pulls from, the
+    # ghost planes' included: the first step needs no exchange (and the
+    # boundary slots a neighbour would send hold nothing yet)
+    exchange_before_first_step = False
 
     def forward_end(self):
         self._diag(self.lib.lbm_slab_inspect)

@@ -162,6 +162,8 @@ class SlabDriver:
       forward_stage(t)                work of step t before the exchange (may be none)
       forward_finish(t)               the rest of step t
       exchange_before_end, forward_end()  (optional) a last exchange and a read of the final state
+      exchange_before_first_step      (optional, default True) False when forward_begin already
+                                      leaves the ghost slots of the initial state filled
       diagnostics() -> (n_states, 5)  partial admission sums of every state: mass, exchange,
                                       min population, max |u|^2, non-finite flag
       responses() -> 8                partial responses of the final state
@@ -196,9 +198,11 @@ class SlabDriver:
 
     def forward(self, steps: int) -> dict:
         self.b.forward_begin()
+        first = getattr(self.b, "exchange_before_first_step", True)
         for t in range(steps):
             self.b.forward_stage(t)
-            self._exchange("state")
+            if t > 0 or first:
+                self._exchange("state")
             self.b.forward_finish(t)
         if getattr(self.b, "exchange_before_end", False):
             # a backend that reduces a state while reading it needs the last halos too
