@@ -145,7 +145,7 @@ bool staged_aligned(const void* base, const int64_t* run0, int nrun, size_t elem
 void set_thread_error(const char* msg);
 
 cudaError_t launch_init(int Q, int storage, const Geometry& G, const Physics& P, void* pop, const uint32_t* mask,
-                        cudaStream_t s);
+                        int64_t c_begin, int64_t c_end, cudaStream_t s);  // cells [c_begin, c_end)
 cudaError_t launch_forward(int Q, int coll, int storage, const FwdArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_adjoint(int Q, int coll, int lstorage, const AdjArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_wait_probe(int* err, uint64_t limit_ns, unsigned long long* waited_ns, cudaStream_t s);

@@ -15,12 +15,15 @@ namespace {
 // w(1 - 1.5 c.a), solid w.  Fluid cells scatter through the inverse pull,
 // solid cells fill their own slots.
 template <int Q, typename T>
-__global__ void __launch_bounds__(BLOCK) k_init(Geometry G, Physics P, T* A, const uint32_t* __restrict__ mask) {
+__global__ void __launch_bounds__(BLOCK) k_init(Geometry G, Physics P, T* A, const uint32_t* __restrict__ mask,
+                                                uint32_t c_begin, uint32_t c_end) {
     using L = Lat<Q>;
-    const uint32_t n = (uint32_t)G.n;
-    for (uint32_t x = blockIdx.x * BLOCK + threadIdx.x; x < n; x += gridDim.x * BLOCK) {
+    // an x-slab initialises its owned cells only: they also fill the ghost
+    // slots they pull from, which the ghost cells must not overwrite
+    for (uint32_t x = c_begin + blockIdx.x * BLOCK + threadIdx.x; x < c_end; x += gridDim.x * BLOCK) {
         const uint32_t m = mask[x];
         const bool solid = m & MASK_SOLID;
+        const uint32_t n = (uint32_t)G.n;
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const float ca = L::cx(q) * P.a[0] + L::cy(q) * P.a[1] + L::cz(q) * P.a[2];
@@ -461,12 +464,13 @@ __global__ void __launch_bounds__(BLOCK) k_filter_transpose(DesignArgs a) {
 }  // namespace
 
 cudaError_t launch_init(int Q, int storage, const Geometry& G, const Physics& P, void* pop, const uint32_t* mask,
-                        cudaStream_t s) {
-    const int grid = blocks_for(G.n, 0);
+                        int64_t c_begin, int64_t c_end, cudaStream_t s) {
+    const int grid = blocks_for(c_end - c_begin, 0);
+    const uint32_t b = (uint32_t)c_begin, e = (uint32_t)c_end;
     if (Q == 19) {
-        LBM_STORAGE_DISPATCH(storage, T, k_init<19, T><<<grid, BLOCK, 0, s>>>(G, P, static_cast<T*>(pop), mask))
+        LBM_STORAGE_DISPATCH(storage, T, k_init<19, T><<<grid, BLOCK, 0, s>>>(G, P, static_cast<T*>(pop), mask, b, e))
     } else {
-        LBM_STORAGE_DISPATCH(storage, T, k_init<27, T><<<grid, BLOCK, 0, s>>>(G, P, static_cast<T*>(pop), mask))
+        LBM_STORAGE_DISPATCH(storage, T, k_init<27, T><<<grid, BLOCK, 0, s>>>(G, P, static_cast<T*>(pop), mask, b, e))
     }
     return cudaGetLastError();
 }

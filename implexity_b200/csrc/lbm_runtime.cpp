@@ -902,8 +902,10 @@ void inspect(lbm_handle& h, StepDiag* diag, float* record, bool record_s = false
 
 void init_state(lbm_handle& h) {
     // both arrays: solid cells keep their populations in either
-    CK(launch_init(h.Q, h.storage, h.G, h.P, h.popA(), h.mask.as<uint32_t>(), h.stream));
-    CK(launch_init(h.Q, h.storage, h.G, h.P, h.popB(), h.mask.as<uint32_t>(), h.stream));
+    const int64_t c0 = h.slab ? (int64_t)h.slab_hl * h.G.sx : 0;
+    const int64_t c1 = h.slab ? (int64_t)(h.slab_hl + h.slab_own) * h.G.sx : h.n();
+    CK(launch_init(h.Q, h.storage, h.G, h.P, h.popA(), h.mask.as<uint32_t>(), c0, c1, h.stream));
+    CK(launch_init(h.Q, h.storage, h.G, h.P, h.popB(), h.mask.as<uint32_t>(), c0, c1, h.stream));
     h.pending = false;
     h.t = 0;
     h.state_valid = true;
