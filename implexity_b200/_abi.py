@@ -9,7 +9,7 @@ import ctypes as C
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "liblbm_b200.so"
-ABI_VERSION = 5
+ABI_VERSION = 6
 
 # status codes
 LBM_OK, LBM_E_CONTRACT, LBM_E_CONVERGENCE, LBM_E_CUDA, LBM_E_STATE = 0, 1, 2, 3, 4
@@ -76,6 +76,7 @@ class Port(C.Structure):
         ("frequency_hz", C.c_double),
         ("phase_rad", C.c_double),
         ("ramp_s", C.c_double),
+        ("reconstruction", C.c_int32),
     ]
 
 

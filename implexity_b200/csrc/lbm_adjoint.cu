@@ -132,7 +132,22 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
                     }
                 }
                 a.abar[x] = fmaf(ab, a.abar_factor, ab_prev);
-                if (a.port_transpose && (m & MASK_PORT)) port_transpose<Q>(a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], v);
+                if (a.port_transpose && (m & MASK_PORT)) {
+                    const PortMap& pm = a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1];
+                    if (!pm.recon) {
+                        port_transpose<Q>(pm, v);
+                    } else {
+                        // the neighbour's share stays in this cell's slots until
+                        // the move that follows the step (launch_nee_move); the
+                        // neighbour's (rho, j / rho) from the record (zero
+                        // acceleration: u = j / (rho (1 + alpha / 2)))
+                        const uint32_t xn = (uint32_t)((int64_t)x + pm.nb_off);
+                        const float sc = 1.f + 0.5f * a.alpha[xn];
+                        const float un[3] = {a.record[(size_t)n + xn] * sc, a.record[2 * (size_t)n + xn] * sc,
+                                             a.record[3 * (size_t)n + xn] * sc};
+                        nee_transpose<Q>(pm, a.record[xn], un, v);
+                    }
+                }
                 store_own_lam<Q, T>(D, n, x, v, k_out);
                 if (a.norm2) {
 #pragma unroll

@@ -100,6 +100,15 @@ struct PortMap {
     float dp_weight;        // +1/n_inlet (velocity port), -1/n_outlet (pressure port)
     float bias[27];
     float jac[27][27];      // rows of the unknown populations
+    // extrapolating ports (recon != 0): every population from the inward
+    // neighbour x + nb_off, f = eq(rho_b, u_b) + f_n - eq(rho_n, u_n), where
+    // rho_b = rho_n when rb_nb, else 1 + rb1, and u_b[d] = u_n[d] where bit d
+    // of ub_nb is set, else u_port[d]
+    int32_t recon;
+    int32_t nb_off;
+    int32_t rb_nb, ub_nb;
+    float rb1;
+    float u_port[3];
 };
 
 // ------------------------------------------------------------------ arguments

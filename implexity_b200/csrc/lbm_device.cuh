@@ -274,6 +274,133 @@ __device__ __forceinline__ void port_transpose(const PortMap& P, float (&v)[Q]) 
     }
 }
 
+// ------------------------------------------------------------------ extrapolating ports
+// Non-equilibrium extrapolation from the inward neighbour x + nb_off
+// (ports.rs reconstruct_neighbor :484-497; moving/boundary.rs
+// port_populations :445-458): f = eq(rho_b, u_b) + f_n - eq(rho_n, u_n) with
+// u_n = j_n / rho_n.  In shifted variables g = f - w the weights cancel:
+// g = g_n + eq(rho_b, u_b) - eq(rho_n, u_n).  R is float or double.
+template <typename R>
+__device__ __forceinline__ void nee_targets(const PortMap& P, R rp_n, const R (&u_n)[3], R& rp_b, R (&u_b)[3]) {
+    rp_b = P.rb_nb ? rp_n : (R)P.rb1;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) u_b[d] = ((P.ub_nb >> d) & 1) ? u_n[d] : (R)P.u_port[d];
+}
+
+template <int Q, typename R>
+__device__ __forceinline__ void nee_moments(const R (&gn)[Q], R& rp, R (&u)[3]) {
+    using L = Lat<Q>;
+    R j[3] = {0, 0, 0};
+    rp = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        rp += gn[q];
+        if (L::cx(q)) j[0] += L::cx(q) * gn[q];
+        if (L::cy(q)) j[1] += L::cy(q) * gn[q];
+        if (L::cz(q)) j[2] += L::cz(q) * gn[q];
+    }
+    const R inv = (R)1 / ((R)1 + rp);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) u[d] = j[d] * inv;
+}
+
+// out <- the port cell's populations from the neighbour's streamed gn.
+template <int Q, typename R>
+__device__ __forceinline__ void nee_apply(const PortMap& P, const R (&gn)[Q], R (&out)[Q]) {
+    using L = Lat<Q>;
+    R rp, u[3], rb, ub[3];
+    nee_moments<Q, R>(gn, rp, u);
+    nee_targets<R>(P, rp, u, rb, ub);
+    const R rho = (R)1 + rp, rho_b = (R)1 + rb;
+    const R u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2], ub2 = ub[0] * ub[0] + ub[1] * ub[1] + ub[2] * ub[2];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const R cb = L::cx(q) * ub[0] + L::cy(q) * ub[1] + L::cz(q) * ub[2];
+        const R cn = L::cx(q) * u[0] + L::cy(q) * u[1] + L::cz(q) * u[2];
+        // eq_b - eq_n = w [(rho_b - rho_n) + rho_b (3 cb + 4.5 cb^2 - 1.5 ub^2) - rho_n (...)]
+        const R d = (rb - rp) + rho_b * (3 * cb + (R)4.5 * cb * cb - (R)1.5 * ub2) -
+                    rho * (3 * cn + (R)4.5 * cn * cn - (R)1.5 * u2);
+        out[q] = gn[q] + (R)L::wd(q) * d;
+    }
+}
+
+// v <- the cotangent of the neighbour's streamed populations given v, the
+// cotangent of the port cell's populations, at the neighbour's (rho - 1, u)
+// (port_populations_vjp, moving/boundary.rs:462-506, with
+// equilibrium_vjp; the neighbor_non_equilibrium port's axial velocity
+// follows the neighbour's the same way).
+template <int Q>
+__device__ __forceinline__ void nee_transpose(const PortMap& P, float rp_n, const float (&u_n)[3], float (&v)[Q]) {
+    using L = Lat<Q>;
+    float rb, ub[3];
+    nee_targets<float>(P, rp_n, u_n, rb, ub);
+    const float rho_n = 1.f + rp_n, rho_b = 1.f + rb;
+    const float un2 = u_n[0] * u_n[0] + u_n[1] * u_n[1] + u_n[2] * u_n[2];
+    const float ub2 = ub[0] * ub[0] + ub[1] * ub[1] + ub[2] * ub[2];
+    float rbb = 0.f, rnb = 0.f, ubb[3] = {0.f, 0.f, 0.f}, unb[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const float g = v[q] * L::w(q);
+        const float cb = L::cx(q) * ub[0] + L::cy(q) * ub[1] + L::cz(q) * ub[2];
+        const float cn = L::cx(q) * u_n[0] + L::cy(q) * u_n[1] + L::cz(q) * u_n[2];
+        rbb += g * (1.f + 3.f * cb + 4.5f * cb * cb - 1.5f * ub2);
+        rnb -= g * (1.f + 3.f * cn + 4.5f * cn * cn - 1.5f * un2);
+        const float c[3] = {(float)L::cx(q), (float)L::cy(q), (float)L::cz(q)};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            ubb[d] += g * (3.f * c[d] + 9.f * cb * c[d] - 3.f * ub[d]);
+            unb[d] -= g * (3.f * c[d] + 9.f * cn * c[d] - 3.f * u_n[d]);
+        }
+    }
+    if (P.rb_nb) rnb += rbb;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        ubb[d] *= rho_b;
+        unb[d] *= rho_n;
+        if ((P.ub_nb >> d) & 1) unb[d] += ubb[d];
+    }
+    // u_n = j / rho_n: j_bar = u_bar / rho_n, rho_bar -= u_bar . u_n / rho_n
+    const float inv = 1.f / rho_n;
+    float jb[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        jb[d] = unb[d] * inv;
+        rnb -= unb[d] * u_n[d] * inv;
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) v[q] += rnb + L::cx(q) * jb[0] + L::cy(q) * jb[1] + L::cz(q) * jb[2];
+}
+
+// The post-port populations g of port cell x (shifted) from the population
+// array A: the legacy affine map on its own streamed g, or the extrapolation
+// from the inward neighbour's streamed populations (read through the same
+// pull).  Returns the exchanged mass; rp_n / u_n receive the neighbour's
+// (rho - 1, j / rho) for the extrapolating ports.
+template <int Q, typename T>
+__device__ __forceinline__ float port_state(const PortMap& P, const T* __restrict__ A, const Geometry& G,
+                                            const uint32_t* __restrict__ mask, uint32_t x, float (&g)[Q],
+                                            float* rp_n = nullptr, float* u_n = nullptr) {
+    if (!P.recon) return apply_port<Q>(P, g);
+    const uint32_t xn = (uint32_t)((int64_t)x + P.nb_off);
+    float gn[Q], out[Q];
+    load_pop<Q, T>(A, G, xn, mask[xn], gn);
+    nee_apply<Q, float>(P, gn, out);
+    if (rp_n) {
+        float u[3];
+        nee_moments<Q, float>(gn, *rp_n, u);
+        u_n[0] = u[0];
+        u_n[1] = u[1];
+        u_n[2] = u[2];
+    }
+    float exch = 0.f;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        exch += out[q] - g[q];
+        g[q] = out[q];
+    }
+    return exch;
+}
+
 // ------------------------------------------------------------------ physics
 struct Macro {
     float rp, rho, u[3], F[3];

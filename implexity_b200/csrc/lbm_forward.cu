@@ -2,7 +2,8 @@
 //
 // One launch = one time step of the whole grid: pull from the current array
 // (Streaming::stream with halfway bounce-back, solver.rs:131-157) -> port
-// reconstruction (ports.rs:560-579) -> admission reductions of the streamed
+// reconstruction (ports.rs:560-579; an extrapolating port cell pulls its
+// inward neighbour's populations as well) -> admission reductions of the streamed
 // state (solver.rs:714-755) -> optional (rho, u) record for the adjoint ->
 // collision (BGK/TRT/MRT with Guo-Brinkman forcing) -> aligned store into the
 // cell's own slots of the other array.  The pulled runs are staged through
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(TPB, (Q == 19 ? 3 : 2)) k_forward(FwdArgs a) {
 #pragma unroll
                         for (int q = 0; q < Q; ++q) v[q] *= L::w(q);
                     }
-                    exch = apply_port<Q>(a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], v);
+                    exch = port_state<Q, T>(a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], A, a.G, a.mask, x, v);
                     if constexpr (SC) {
 #pragma unroll
                         for (int q = 0; q < Q; ++q) v[q] *= (float)(1.0 / L::wd(q));

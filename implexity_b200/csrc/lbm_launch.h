@@ -171,9 +171,15 @@ cudaError_t launch_halo_copy(int storage, void* arr, int64_t n, int64_t plane0, 
                              int ndir, void* buf, int unpack, cudaStream_t s);
 cudaError_t launch_canon_lam(int Q, int lstorage, const Geometry& G, const void* lam, const uint32_t* mask,
                              float inv_scale, float* out, int grid, cudaStream_t s);
+// rec_next: the (rho-1, u) record of the state lambda belongs to (read at
+// the neighbours of extrapolating port cells; nullptr without such ports)
 cudaError_t launch_seed_lam(int Q, int lstorage, const Geometry& G, void* lam, const uint32_t* mask,
-                            const PortMap* ports, const float* in, float scale, int port_transpose, int grid,
-                            cudaStream_t s);
+                            const PortMap* ports, const float* in, float scale, int port_transpose,
+                            const float* rec_next, const float* alpha, int grid, cudaStream_t s);
+// Moves the neighbour's share of one extrapolating port's cotangents
+// (left in the port cells' slots) into the neighbours' slots.
+cudaError_t launch_nee_move(int lstorage, void* lam, int64_t n, int Q, const uint32_t* cells, int64_t count,
+                            int64_t nb_off, cudaStream_t s);
 cudaError_t launch_design_map(const DesignArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_sens_scale(const DesignArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_filter_transpose(const DesignArgs& a, int grid, cudaStream_t s);

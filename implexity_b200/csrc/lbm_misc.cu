@@ -67,7 +67,16 @@ __global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
             double gd[Q];
 #pragma unroll
             for (int q = 0; q < Q; ++q) gd[q] = g[q];
-            if (a.apply_ports && pm) {
+            if (a.apply_ports && pm && pm->recon) {
+                // extrapolation from the inward neighbour's streamed populations
+                const uint32_t xn = (uint32_t)((int64_t)x + pm->nb_off);
+                float gnf[Q];
+                load_pop<Q, T>(A, a.G, xn, a.mask[xn], gnf);
+                double gn[Q];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) gn[q] = gnf[q];
+                nee_apply<Q, double>(*pm, gn, gd);
+            } else if (a.apply_ports && pm) {
                 double in[Q];
 #pragma unroll
                 for (int q = 0; q < Q; ++q) in[q] = gd[q];
@@ -130,7 +139,20 @@ __global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
             }
             continue;
         }
-        if (a.apply_ports && pm) apply_port<Q>(*pm, g);
+        // the neighbour's (rho - 1, j / rho) of an extrapolating port cell
+        float rpn = 0.f, un[3] = {0.f, 0.f, 0.f};
+        if (pm && pm->recon && (a.apply_ports || a.port_transpose)) {
+            float gp[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) gp[q] = g[q];
+            port_state<Q, T>(*pm, A, a.G, a.mask, x, gp, &rpn, un);
+            if (a.apply_ports) {
+#pragma unroll
+                for (int q = 0; q < Q; ++q) g[q] = gp[q];
+            }
+        } else if (a.apply_ports && pm) {
+            apply_port<Q>(*pm, g);
+        }
         Macro M = macroscopic<Q>(g, alpha, a.P);
         float S[6];
         second_moments<Q>(g, S);
@@ -153,7 +175,12 @@ __global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
                 a.record[2 * n + x] = u[1];
                 a.record[3 * n + x] = u[2];
             }
-            if (a.port_transpose && pm) port_transpose<Q>(*pm, fb);
+            // (an extrapolating port cell keeps its neighbour's share in its own
+            // slots for launch_nee_move)
+            if (a.port_transpose && pm) {
+                if (pm->recon) nee_transpose<Q>(*pm, rpn, un, fb);
+                else port_transpose<Q>(*pm, fb);
+            }
             if (a.write_lambda) {
                 TL* B = static_cast<TL*>(a.lam);
 #pragma unroll
@@ -192,7 +219,7 @@ __global__ void __launch_bounds__(BLOCK) k_canon_pop(Geometry G, const T* A, con
             for (int q = 0; q < Q; ++q) g[q] = pdec<Q, T>(A[(int64_t)q * G.n + x], q);
         } else {
             load_pop<Q, T>(A, G, x, m, g);
-            if (apply_ports && (m & MASK_PORT)) apply_port<Q>(ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], g);
+            if (apply_ports && (m & MASK_PORT)) port_state<Q, T>(ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], A, G, mask, x, g);
         }
 #pragma unroll
         for (int q = 0; q < Q; ++q) out[(int64_t)q * G.n + x] = g[q];
@@ -226,19 +253,52 @@ __global__ void __launch_bounds__(BLOCK) k_canon_lam(Geometry G, const T* B, con
 }
 
 // Natural lambda (cotangent of the post-port state) -> stored seed layout.
+// Extrapolating port cells take the neighbour's (rho - 1, u) from rec_next,
+// the record of the state lambda belongs to, and keep the neighbour's share
+// in their own slots for launch_nee_move.
 template <int Q, typename T>
 __global__ void __launch_bounds__(BLOCK) k_seed_lam(Geometry G, T* B, const uint32_t* __restrict__ mask,
                                                     const PortMap* ports, const float* in, float scale,
-                                                    int port_transpose_on) {
+                                                    int port_transpose_on, const float* rec_next,
+                                                    const float* __restrict__ alpha) {
     for (int64_t x = (int64_t)blockIdx.x * BLOCK + threadIdx.x; x < G.n; x += (int64_t)gridDim.x * BLOCK) {
         const uint32_t m = mask[x];
         if (m & MASK_SOLID) continue;
         float v[Q];
 #pragma unroll
         for (int q = 0; q < Q; ++q) v[q] = in[(int64_t)q * G.n + x];
-        if (port_transpose_on && (m & MASK_PORT)) port_transpose<Q>(ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], v);
+        if (port_transpose_on && (m & MASK_PORT)) {
+            const PortMap& pm = ports[((m >> MASK_PORT_SHIFT) & 7u) - 1];
+            if (!pm.recon) {
+                port_transpose<Q>(pm, v);
+            } else {
+                const int64_t xn = x + pm.nb_off;
+                const float sc = 1.f + 0.5f * alpha[xn];
+                const float un[3] = {rec_next[G.n + xn] * sc, rec_next[2 * G.n + xn] * sc, rec_next[3 * G.n + xn] * sc};
+                nee_transpose<Q>(pm, rec_next[xn], un, v);
+            }
+        }
 #pragma unroll
         for (int q = 0; q < Q; ++q) B[q * G.n + x] = Cvt<T>::from(v[q] * scale);
+    }
+}
+
+// Second half of an extrapolating port's transpose: the neighbour's share,
+// which the transposed step (or seed) left in the port cell's own slots, is
+// added to the neighbour's slots and the port cell's slots are cleared
+// (its populations are rebuilt from the neighbour, so nothing flows back
+// through them).  The cells of one port have distinct neighbours; ports are
+// moved one launch after another.
+template <typename TL>
+__global__ void __launch_bounds__(BLOCK) k_nee_move(TL* B, int64_t n, int Q, const uint32_t* __restrict__ cells,
+                                                   int64_t count, int64_t nb_off) {
+    for (int64_t i = (int64_t)blockIdx.x * BLOCK + threadIdx.x; i < count; i += (int64_t)gridDim.x * BLOCK) {
+        const int64_t x = cells[i], xn = x + nb_off;
+        for (int q = 0; q < Q; ++q) {
+            const float v = Cvt<TL>::to(B[q * n + x]);
+            B[q * n + xn] = Cvt<TL>::from(Cvt<TL>::to(B[q * n + xn]) + v);
+            B[q * n + x] = Cvt<TL>::from(0.f);
+        }
     }
 }
 
@@ -260,7 +320,7 @@ __global__ void __launch_bounds__(BLOCK) k_wall_loads(Geometry G, Physics P, con
         const uint32_t m = mask[x];
         float g[Q];
         load_pop<Q, T>(A, G, x, m, g);
-        if (apply_ports && (m & MASK_PORT)) apply_port<Q>(ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], g);
+        if (apply_ports && (m & MASK_PORT)) port_state<Q, T>(ports[((m >> MASK_PORT_SHIFT) & 7u) - 1], A, G, mask, x, g);
         const float om = omega_cell ? omega_cell[x] : P.omega;  // BGK: both pair rates
         collide_fused<Q, CK_PAIRS, 0>(g, alpha[x], P, true, om, om);
         float o = 0.f;
@@ -583,17 +643,26 @@ cudaError_t launch_canon_lam(int Q, int lstorage, const Geometry& G, const void*
 }
 
 cudaError_t launch_seed_lam(int Q, int lstorage, const Geometry& G, void* lam, const uint32_t* mask,
-                            const PortMap* ports, const float* in, float scale, int port_transpose_on, int grid,
-                            cudaStream_t s) {
+                            const PortMap* ports, const float* in, float scale, int port_transpose_on,
+                            const float* rec_next, const float* alpha, int grid, cudaStream_t s) {
     if (Q == 19) {
         LBM_STORAGE_DISPATCH(lstorage, T,
                              k_seed_lam<19, T><<<grid, BLOCK, 0, s>>>(G, static_cast<T*>(lam), mask, ports, in,
-                                                                       scale, port_transpose_on))
+                                                                       scale, port_transpose_on, rec_next, alpha))
     } else {
         LBM_STORAGE_DISPATCH(lstorage, T,
                              k_seed_lam<27, T><<<grid, BLOCK, 0, s>>>(G, static_cast<T*>(lam), mask, ports, in,
-                                                                       scale, port_transpose_on))
+                                                                       scale, port_transpose_on, rec_next, alpha))
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_nee_move(int lstorage, void* lam, int64_t n, int Q, const uint32_t* cells, int64_t count,
+                            int64_t nb_off, cudaStream_t s) {
+    if (count <= 0) return cudaSuccess;
+    const int grid = (int)std::min<int64_t>((count + BLOCK - 1) / BLOCK, 1024);
+    LBM_STORAGE_DISPATCH(lstorage, T,
+                         k_nee_move<T><<<grid, BLOCK, 0, s>>>(static_cast<T*>(lam), n, Q, cells, count, nb_off))
     return cudaGetLastError();
 }
 

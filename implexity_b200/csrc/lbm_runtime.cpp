@@ -172,6 +172,8 @@ struct PortSpec {
     double mean_vel[3] = {0, 0, 0}, amp_vel[3] = {0, 0, 0};  // lattice units
     double mean_rho = 1.0, amp_rho = 0.0;                     // lattice density (mean includes 1)
     double freq = 0, phase = 0, ramp = 0;
+    int recon = LBM_RECON_LEGACY_MOMENT;  // lbm_port_reconstruction
+    int64_t nb_off = 0;                   // inward neighbour offset (extrapolating ports)
 };
 
 // Signal::factors (moving/boundary.rs:111-125): the C2 smoothstep ramp and
@@ -369,6 +371,10 @@ struct lbm_handle {
     std::vector<uint32_t> wall_cells;
     std::vector<uint8_t> wall_links;
     DevBuf wall_cells_d, wall_links_d, wall_out;
+    // cells of the extrapolating ports, grouped by port: (first, count,
+    // port) per group; their transposes move cotangents to the neighbours
+    std::vector<std::array<int64_t, 3>> nee_groups;
+    DevBuf nee_cells_d;
     // --- state
     bool design_set = false, state_valid = false, forward_done = false;
     int cur = 0;   // which population array holds the current state
@@ -450,6 +456,17 @@ std::vector<PortMap> port_maps_at(const lbm_handle& h, double t_s) {
             reconstruct(h.L, spec, h.a, pert, r1);
             for (int r = 0; r < Q; ++r)
                 if (M.unknown_mask & (1u << r)) M.jac[r][kq] = (float)(r1[r] - r0[r]);
+        }
+        // extrapolating ports: which of the boundary density / velocity the
+        // neighbour supplies (ports.rs:484-497, moving/boundary.rs:445-458)
+        M.recon = spec.recon;
+        if (spec.recon != LBM_RECON_LEGACY_MOMENT) {
+            M.nb_off = (int32_t)spec.nb_off;
+            const bool neighbor = spec.recon == LBM_RECON_NEIGHBOR_NON_EQUILIBRIUM;
+            M.rb_nb = (!neighbor && !spec.pressure) ? 1 : 0;
+            M.ub_nb = neighbor ? (1 << spec.axis) : (spec.pressure ? 7 : 0);
+            M.rb1 = (float)(spec.density - 1.0);
+            for (int d = 0; d < 3; ++d) M.u_port[d] = (float)spec.vel[d];
         }
         const int64_t ni = h.global_inlet >= 0 ? h.global_inlet : h.n_inlet;
         const int64_t no = h.global_outlet >= 0 ? h.global_outlet : h.n_outlet;
@@ -647,6 +664,27 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
         for (int64_t x : cells)
             require(!(p.solid_mask[x] || p.design_region[x] || p.fixed_design[x] != 1.0),
                     "Port cells must be protected, unobstructed, fixed-design fluid");
+        // reconstruction (ports.rs:134-157, 202-219)
+        require(pt.reconstruction >= LBM_RECON_LEGACY_MOMENT && pt.reconstruction <= LBM_RECON_NON_EQUILIBRIUM_EXTRAPOLATION,
+                "Port reconstruction must be legacy_moment, neighbor_non_equilibrium or non_equilibrium_extrapolation");
+        s.recon = pt.reconstruction;
+        const bool accelerated = p.acceleration_m_s2[0] != 0.0 || p.acceleration_m_s2[1] != 0.0 ||
+                                 p.acceleration_m_s2[2] != 0.0;
+        require(!(s.recon == LBM_RECON_NEIGHBOR_NON_EQUILIBRIUM && (!s.pressure || accelerated)),
+                "neighbor_non_equilibrium currently requires a pressure port and zero acceleration");
+        require(!(s.recon == LBM_RECON_NON_EQUILIBRIUM_EXTRAPOLATION && accelerated),
+                "non_equilibrium_extrapolation requires zero acceleration");
+        if (s.recon != LBM_RECON_LEGACY_MOMENT) {
+            require(shape[s.axis] >= 2, "Neighbor pressure reconstruction requires an inward fluid plane");
+            const int64_t stride[3] = {h.G.sx, h.G.sy, 1};
+            s.nb_off = s.sign * stride[s.axis];
+            for (int64_t x : cells) {
+                const int64_t y = x + s.nb_off;
+                require(!(p.solid_mask[y] || p.design_region[y] || p.fixed_design[y] != 1.0),
+                        "Neighbor pressure reconstruction requires protected, unobstructed, fixed-design inward fluid "
+                        "cells");
+            }
+        }
         for (int d = 0; d < 3; ++d)
             require(std::isfinite(pt.velocity_m_s[d]), "Port velocity requires three finite components");
         for (int d = 0; d < 3; ++d) s.vel[d] = pt.velocity_m_s[d] * p.step_s / p.spacing_m;
@@ -688,6 +726,12 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
         port_cells.push_back(cells);
     }
     h.n_ports = (int)specs.size();
+    // an extrapolating port reads its neighbours' streamed populations, which
+    // must not be rebuilt by a port themselves
+    for (size_t k = 0; k < specs.size(); ++k)
+        if (specs[k].recon != LBM_RECON_LEGACY_MOMENT)
+            for (int64_t x : port_cells[k])
+                require(!used[x + specs[k].nb_off], "The inward neighbours of an extrapolating port cannot be port cells");
     h.n_inlet = h.n_outlet = 0;
     for (size_t k = 0; k < specs.size(); ++k) (specs[k].pressure ? h.n_outlet : h.n_inlet) += (int64_t)port_cells[k].size();
 
@@ -727,6 +771,13 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
     }
     for (size_t k = 0; k < port_cells.size(); ++k)
         for (int64_t x : port_cells[k]) mask[x] |= (uint32_t)(k + 1) << MASK_PORT_SHIFT;
+    std::vector<uint32_t> nee_cells;
+    h.nee_groups.clear();
+    for (size_t k = 0; k < port_cells.size(); ++k) {
+        if (specs[k].recon == LBM_RECON_LEGACY_MOMENT) continue;
+        h.nee_groups.push_back({(int64_t)nee_cells.size(), (int64_t)port_cells[k].size(), (int64_t)k});
+        for (int64_t x : port_cells[k]) nee_cells.push_back((uint32_t)x);
+    }
 
     // wall links of the momentum-exchange loads (wall_exchange.rs:44-70): every
     // blocked pull link of a fluid cell, cells and links in order, except the
@@ -818,6 +869,11 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
     if (!h.offsets.empty())
         CK(cudaMemcpyAsync(h.offsets_d.p, h.offsets.data(), h.offsets.size() * sizeof(int4), cudaMemcpyHostToDevice,
                            h.stream));
+    if (!nee_cells.empty()) {
+        h.nee_cells_d.alloc(nee_cells.size() * sizeof(uint32_t), ctr);
+        CK(cudaMemcpyAsync(h.nee_cells_d.p, nee_cells.data(), nee_cells.size() * sizeof(uint32_t),
+                           cudaMemcpyHostToDevice, h.stream));
+    }
     if (!maps.empty())
         CK(cudaMemcpyAsync(h.ports_d.p, maps.data(), maps.size() * sizeof(PortMap), cudaMemcpyHostToDevice,
                            h.stream));
@@ -1141,6 +1197,14 @@ struct AdjState {
     int64_t steps = 0;
 };
 
+// Second half of the extrapolating ports' transposes on the cotangent array
+// `lam` (launch_nee_move), one port after another.
+void nee_move(lbm_handle& h, void* lam, int lam_storage) {
+    for (const auto& g : h.nee_groups)
+        CK(launch_nee_move(lam_storage, lam, h.n(), h.Q, h.nee_cells_d.as<uint32_t>() + g[0], g[1],
+                           h.port_specs[(size_t)g[2]].nb_off, h.stream));
+}
+
 AdjArgs adj_args(lbm_handle& h) {
     AdjArgs a{};
     a.G = h.G;
@@ -1176,6 +1240,7 @@ void adjoint_step(lbm_handle& h, AdjState& st, const float* rec, bool want_norm,
     a.norm2 = want_norm ? h.norm2.as<double>() : nullptr;
     CK(launch_adjoint(h.Q, coll_kernel(h), h.lam_storage, a, grid_for(h), h.stream));
     h.lcur ^= 1;
+    nee_move(h, h.lamA(), h.lam_storage);
     st.scale = st.target;
     st.first = false;
     ++st.steps;
@@ -1248,6 +1313,7 @@ double seed(lbm_handle& h, const double* w, AdjState& st, float* record, double 
     a.norm2 = nullptr;
     a.record = nullptr;
     CK(launch_objective(h.Q, h.storage, h.lam_storage, 1, a, grid_for(h), h.stream));
+    nee_move(h, h.lamA(), h.lam_storage);
     st.first = true;
     return n0;
 }
@@ -2146,6 +2212,21 @@ lbm_status step_vjp_impl(lbm_handle* h, const double* state, const double* lambd
     }
     alloc_adjoint(*h, LBM_STORE_F32);
     h->record.alloc(((size_t)N * 4 + CELL_PAD) * sizeof(float), ctr);
+    // extrapolating ports transpose at the neighbours of the next state:
+    // its (rho - 1, u) record from one step into the other array, which
+    // leaves the current one (this state) in place
+    DevBuf rec_next;
+    if (!h->nee_groups.empty()) {
+        rec_next.alloc(((size_t)N * 4 + CELL_PAD) * sizeof(float), ctr);
+        const int cur = h->cur;
+        const int64_t t0 = h->t;
+        const bool pend = h->pending;
+        step(*h, nullptr, nullptr);
+        inspect(*h, nullptr, rec_next.as<float>());
+        h->cur = cur;
+        h->t = t0;
+        h->pending = pend;
+    }
     inspect(*h, nullptr, h->record.as<float>());
     std::vector<float> v((size_t)N * Q);
     for (int64_t x = 0; x < N; ++x)
@@ -2153,7 +2234,9 @@ lbm_status step_vjp_impl(lbm_handle* h, const double* state, const double* lambd
     ensure_scratch(*h);
     CK(cudaMemcpyAsync(h->scratch.p, v.data(), v.size() * 4, cudaMemcpyHostToDevice, h->stream));
     CK(launch_seed_lam(Q, LBM_STORE_F32, h->G, h->lamA(), h->mask.as<uint32_t>(), ports_at(*h, h->t + 1),
-                       h->scratch.as<float>(), 1.f, 1, grid_for(*h), h->stream));
+                       h->scratch.as<float>(), 1.f, 1, rec_next.as<float>(), h->alpha.as<float>(), grid_for(*h),
+                       h->stream));
+    nee_move(*h, h->lamA(), LBM_STORE_F32);
     if (tau_bar)
         CK(launch_tau_bar(Q, h->G, h->P, h->tau_state.as<float>(), static_cast<const float*>(h->lamA()),
                           h->mask.as<uint32_t>(), h->alpha.as<float>(),
@@ -2244,6 +2327,8 @@ lbm_status lbm_create_slab(const lbm_problem_t* problem, int32_t x_begin, int32_
             const lbm_port_t& pt = P.ports[k];
             require(pt.mask != nullptr, "Port mask must be a shape-matched boolean array");
             require(pt.face == LBM_XMIN || pt.face == LBM_XMAX, "x-slab decomposition supports ports on the x faces only");
+            require(pt.reconstruction == LBM_RECON_LEGACY_MOMENT,
+                    "x-slab decomposition supports legacy_moment ports only");
             int64_t cnt = 0;
             for (int64_t x = 0; x < ng; ++x) cnt += pt.mask[x] ? 1 : 0;
             (pt.kind == LBM_PORT_PRESSURE ? gout : gin) += cnt;

@@ -41,6 +41,8 @@ PROBLEM_KEYS = sorted(
         "step_s",
     ]
 )
+# port reconstructions (ports.rs:134-147) and the moving engine's extrapolation (moving/boundary.rs:445-506)
+RECONSTRUCTIONS = {"legacy_moment": 0, "neighbor_non_equilibrium": 1, "non_equilibrium_extrapolation": 2}
 OPTIONAL_KEYS = ["topology_map", "ports", "origin_m", "field_registration", "geometry_source", "solver_options"]
 
 STORAGE = {"float32": _abi.LBM_STORE_F32, "float16": _abi.LBM_STORE_F16, "bfloat16": _abi.LBM_STORE_BF16}
@@ -244,6 +246,7 @@ class NormalizedProblem:
             ports[k].frequency_hz = port.get("frequency_hz", 0.0)
             ports[k].phase_rad = port.get("phase_rad", 0.0)
             ports[k].ramp_s = port.get("ramp_s", 0.0)
+            ports[k].reconstruction = RECONSTRUCTIONS[port.get("reconstruction", "legacy_moment")]
         p.n_ports = len(self.ports)
         p.time_average = 1 if o.time_average else 0
         p.collision_fp64 = 1 if o.collision_arithmetic == "float64" else 0
@@ -270,12 +273,14 @@ def _ports(value: Any, shape: tuple[int, int, int]) -> list[dict]:
         if keys != required or not isinstance(pid, str) or not pid.strip() or pid in ids:
             raise _err("Unique port id and exact port fields required")
         rec = port.get("reconstruction", "legacy_moment")
-        if rec not in ("legacy_moment", "regularized_known_stress", "neighbor_non_equilibrium"):
+        if rec not in ("legacy_moment", "regularized_known_stress", "neighbor_non_equilibrium",
+                       "non_equilibrium_extrapolation"):
             raise _err(
                 "Port reconstruction must be legacy_moment, regularized_known_stress or neighbor_non_equilibrium"
             )
-        if rec != "legacy_moment":
-            raise _err(f"Port reconstruction {rec} is not provided by the GPU provider; use legacy_moment")
+        if rec == "regularized_known_stress":
+            raise _err("Port reconstruction regularized_known_stress is not provided by the GPU provider; use "
+                       "legacy_moment, neighbor_non_equilibrium or non_equilibrium_extrapolation")
         ids.add(pid)
         if port.get("face") not in _abi.FACES:
             raise _err("Port must identify one Cartesian face")
@@ -285,7 +290,8 @@ def _ports(value: Any, shape: tuple[int, int, int]) -> list[dict]:
         vel = np.asarray(port.get("velocity_m_s"), dtype=float) if port.get("velocity_m_s") is not None else None
         if vel is None or vel.shape != (3,) or not np.all(np.isfinite(vel)):
             raise _err("Port velocity requires three finite components")
-        entry = {"id": pid, "kind": kind, "face": port["face"], "mask": mask, "velocity_m_s": [float(x) for x in vel]}
+        entry = {"id": pid, "kind": kind, "face": port["face"], "mask": mask, "velocity_m_s": [float(x) for x in vel],
+                 "reconstruction": rec}
         if kind == "pressure":
             g = _scalar(port.get("gauge_pressure_Pa"))
             if g is None:

@@ -51,7 +51,7 @@
 extern "C" {
 #endif
 
-#define LBM_ABI_VERSION 5
+#define LBM_ABI_VERSION 6
 
 #if defined(__GNUC__)
 #define LBM_API __attribute__((visibility("default")))
@@ -86,6 +86,24 @@ typedef enum { LBM_STORE_F32 = 0, LBM_STORE_F16 = 1, LBM_STORE_BF16 = 2 } lbm_st
 
 typedef enum { LBM_PORT_VELOCITY = 0, LBM_PORT_PRESSURE = 1 } lbm_port_kind;
 
+/* How a port rebuilds its cells' populations after streaming.
+ * LEGACY_MOMENT: the unknown (incoming) populations from the cell's own known
+ *   ones with a least-squares moment correction (ports.rs:343-406).
+ * NEIGHBOR_NON_EQUILIBRIUM: every population from the inward neighbour's,
+ *   f = eq(rho_port, u_t) + f_n - eq(rho_n, u_n), u_t the port velocity with its
+ *   axial component taken from the neighbour (ports.rs:484-497; pressure
+ *   ports only).
+ * NON_EQUILIBRIUM_EXTRAPOLATION: the moving engine's port (moving/boundary.rs:
+ *   445-506), f = eq(rho_b, u_b) + f_n - eq(rho_n, u_n) with (rho_n, u_port) on
+ *   velocity ports and (rho_port, u_n) on pressure ports.
+ * Both extrapolations need zero acceleration (ports.rs:148-157); their
+ * transposes add into the neighbour's cotangent after each transposed step. */
+typedef enum {
+    LBM_RECON_LEGACY_MOMENT = 0,
+    LBM_RECON_NEIGHBOR_NON_EQUILIBRIUM = 1,
+    LBM_RECON_NON_EQUILIBRIUM_EXTRAPOLATION = 2
+} lbm_port_reconstruction;
+
 /* Faces in the order of ports.rs FACES: xmin, xmax, ymin, ymax, zmin, zmax. */
 typedef enum {
     LBM_XMIN = 0, LBM_XMAX = 1, LBM_YMIN = 2, LBM_YMAX = 3, LBM_ZMIN = 4, LBM_ZMAX = 5
@@ -114,8 +132,8 @@ enum {
 
 #define LBM_MAX_PORTS 7
 
-/* One planar port (ports.rs:55-68, normalize_ports :106-272).  Only the
- * default "legacy_moment" reconstruction (ports.rs:343-406) is provided.
+/* One planar port (ports.rs:55-68, normalize_ports :106-272), rebuilt by
+ * the reconstruction `reconstruction` selects.
  *
  * Pulsatile ports follow the moving engine's port signal
  * (moving/boundary.rs:98-126, Signal::factors; value at time t,
@@ -137,6 +155,7 @@ typedef struct {
     double frequency_hz;      /* >= 0 */
     double phase_rad;
     double ramp_s;            /* >= 0 */
+    int32_t reconstruction;   /* lbm_port_reconstruction */
 } lbm_port_t;
 
 /* The problem mapping of solver.rs:46-65 after JSON parsing (key sets and

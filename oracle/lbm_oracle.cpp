@@ -145,6 +145,11 @@ bool make_basis(const Lattice& L, Basis& B) {
 struct Port {
     bool pressure = false;
     int axis = 0, sign = 1;
+    // 0: legacy moment (ports.rs:343-406); 1: neighbor_non_equilibrium
+    // (ports.rs:484-497); 2: the moving engine's non-equilibrium extrapolation
+    // (moving/boundary.rs:445-460).  1 and 2 read the inward neighbour.
+    int recon = 0;
+    int64_t nb_off = 0;
     double vel[3] = {0, 0, 0};  // value in force at the current time
     double density = 1.0;
     std::vector<int64_t> cells;
@@ -364,6 +369,84 @@ void port_jacobian(const orc_problem& o, Port& pt) {
 
 // Port values of the reconstruction that produces state t_index
 // (t = t_index * dt; moving/field.rs:1002-1013): ramp (wave amplitude + mean).
+// Non-equilibrium extrapolation from the inward neighbour's populations nb
+// (f form): out = eq(rho_b, u_b) + nb - eq(rho_n, u_n), u_n = j_n / rho_n.
+// ports.rs reconstruct_neighbor (:484-497, pressure ports): rho_b = the port
+// density, u_b = the port velocity with its axial component taken from u_n.
+// moving/boundary.rs port_populations (:445-460): velocity ports rho_b =
+// rho_n, u_b = the port velocity; pressure ports rho_b = the port density,
+// u_b = u_n.
+void nee_targets(const orc_problem& o, const Port& p, double rho_n, const double u_n[3], double& rho_b, double u_b[3]) {
+    for (int d = 0; d < 3; ++d) u_b[d] = p.vel[d];
+    if (p.recon == 1) {
+        rho_b = p.density;
+        u_b[p.axis] = u_n[p.axis];
+    } else if (p.pressure) {
+        rho_b = p.density;
+        for (int d = 0; d < 3; ++d) u_b[d] = u_n[d];
+    } else {
+        rho_b = rho_n;
+    }
+}
+
+void nee_apply(const orc_problem& o, const Port& p, const double* nb, double* out) {
+    const Lattice& L = o.L;
+    double rho_n, j[3], u_n[3], rho_b, u_b[3];
+    moments(L, nb, rho_n, j);
+    for (int d = 0; d < 3; ++d) u_n[d] = j[d] / rho_n;
+    nee_targets(o, p, rho_n, u_n, rho_b, u_b);
+    const double ub2 = u_b[0] * u_b[0] + u_b[1] * u_b[1] + u_b[2] * u_b[2];
+    const double un2 = u_n[0] * u_n[0] + u_n[1] * u_n[1] + u_n[2] * u_n[2];
+    for (int q = 0; q < L.Q; ++q) {
+        const double cb = dotc(L, q, u_b), cn = dotc(L, q, u_n);
+        const double eb = rho_b * L.w[q] * (1.0 + 3.0 * cb + 4.5 * cb * cb - 1.5 * ub2);
+        const double en = rho_n * L.w[q] * (1.0 + 3.0 * cn + 4.5 * cn * cn - 1.5 * un2);
+        out[q] = eb + nb[q] - en;
+    }
+}
+
+// equilibrium_vjp: cotangents of rho and u of sum_q g_q eq_q(rho, u)
+void eq_vjp(const orc_problem& o, double rho, const double u[3], const double* g, double sign, double& rb,
+            double ub[3]) {
+    const Lattice& L = o.L;
+    const double u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    for (int q = 0; q < L.Q; ++q) {
+        const double gq = sign * g[q], cu = dotc(L, q, u);
+        rb += gq * L.w[q] * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * u2);
+        for (int d = 0; d < 3; ++d) ub[d] += gq * rho * L.w[q] * (3.0 * L.c[q][d] + 9.0 * cu * L.c[q][d] - 3.0 * u[d]);
+    }
+}
+
+// port_populations_vjp (moving/boundary.rs:462-506) for both extrapolations:
+// nb_bar = d out / d nb ^T g at the neighbour populations nb.
+void nee_vjp(const orc_problem& o, const Port& p, const double* nb, const double* g, double* nb_bar) {
+    const Lattice& L = o.L;
+    double rho_n, j[3], u_n[3], rho_b, u_b[3];
+    moments(L, nb, rho_n, j);
+    for (int d = 0; d < 3; ++d) u_n[d] = j[d] / rho_n;
+    nee_targets(o, p, rho_n, u_n, rho_b, u_b);
+    double rb = 0, ub[3] = {0, 0, 0}, rn = 0, un[3] = {0, 0, 0};
+    eq_vjp(o, rho_b, u_b, g, 1.0, rb, ub);
+    eq_vjp(o, rho_n, u_n, g, -1.0, rn, un);
+    if (p.recon == 1) {
+        un[p.axis] += ub[p.axis];
+    } else if (p.pressure) {
+        for (int d = 0; d < 3; ++d) un[d] += ub[d];
+    } else {
+        rn += rb;
+    }
+    double jb[3];
+    for (int d = 0; d < 3; ++d) {
+        jb[d] = un[d] / rho_n;
+        rn -= un[d] * j[d] / (rho_n * rho_n);
+    }
+    for (int q = 0; q < L.Q; ++q) {
+        double v = g[q] + rn;
+        for (int d = 0; d < 3; ++d) v += jb[d] * L.c[q][d];
+        nb_bar[q] = v;
+    }
+}
+
 void set_port_time(const orc_problem& o, int64_t t_index) {
     const double t = (double)t_index * o.dt;
     for (Port& p : o.ports) {
@@ -765,7 +848,8 @@ double interval(const orc_problem& o, const double* before, const double* alpha,
     for (const Port& p : o.ports) {
         for (int64_t cell : p.cells) {
             double vals[27];
-            reconstruct(o, p, after + cell * Q, vals);
+            if (p.recon) nee_apply(o, p, after + (cell + p.nb_off) * Q, vals);
+            else reconstruct(o, p, after + cell * Q, vals);
             for (int q = 0; q < Q; ++q) {
                 exch += vals[q] - after[cell * Q + q];
                 after[cell * Q + q] = vals[q];
@@ -785,12 +869,27 @@ void interval_vjp(const orc_problem& o, const double* before, const double* alph
     for (const Port& p : o.ports)
         for (int64_t cell : p.cells)
             for (int q = 0; q < Q; ++q) refl[cell * Q + q] = 0.0;
+    // the extrapolating ports linearise at the neighbours' streamed
+    // populations of the next state (reflected_cells, solver.rs:617-639)
+    std::vector<double> streamed, post_tmp;
+    bool any_nee = false;
+    for (const Port& p : o.ports) any_nee = any_nee || p.recon != 0;
+    if (any_nee) {
+        streamed.resize((size_t)N * Q);
+        interval(o, before, alpha, streamed.data(), post_tmp);
+    }
     for (const Port& p : o.ports)
         for (int64_t cell : p.cells) {
             const double* g = after_bar + cell * Q;
             bool any = false;
             for (int r = 0; r < Q; ++r) any |= g[r] != 0.0;
             if (!any) continue;
+            if (p.recon) {
+                double nb_bar[27];
+                nee_vjp(o, p, streamed.data() + (cell + p.nb_off) * Q, g, nb_bar);
+                for (int k = 0; k < Q; ++k) refl[(cell + p.nb_off) * Q + k] += nb_bar[k];
+                continue;
+            }
             for (int r = 0; r < Q; ++r) {
                 if (g[r] == 0.0) continue;
                 for (int k = 0; k < Q; ++k) refl[cell * Q + k] += p.jac[r * Q + k] * g[r];
@@ -1225,6 +1324,9 @@ int orc_create(const lbm_problem_t* p, orc_problem** out) {
         pt.pulsatile = pt.freq != 0.0 || pt.ramp != 0.0;
         for (int64_t x = 0; x < N; ++x)
             if (src.mask[x]) pt.cells.push_back(x);
+        pt.recon = src.reconstruction;
+        const int64_t stride[3] = {o->shape[1] * o->shape[2], o->shape[2], 1};
+        pt.nb_off = pt.sign * stride[pt.axis];
         port_jacobian(*o, pt);
         for (int64_t x : pt.cells) o->port_role[x] = pt.pressure ? -1 : 1;
         if (pt.pressure) o->n_outlet += (int64_t)pt.cells.size();
@@ -1489,7 +1591,9 @@ int64_t orc_wall_loads(const orc_problem* o, const double* before, const double*
 }
 
 void orc_port_apply(const orc_problem* o, int port, const double* f_in, double* f_out) {
-    reconstruct(*o, o->ports[port], f_in, f_out);
+    // the extrapolating reconstructions read the inward neighbour's populations
+    if (o->ports[port].recon) nee_apply(*o, o->ports[port], f_in, f_out);
+    else reconstruct(*o, o->ports[port], f_in, f_out);
 }
 
 int orc_gradient(const orc_problem* o, const double* raw, const double* w8, int64_t steps, int mode, int64_t K,
