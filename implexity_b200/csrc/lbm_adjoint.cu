@@ -137,15 +137,16 @@ __global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
                     if (!pm.recon) {
                         port_transpose<Q>(pm, v);
                     } else {
-                        // the neighbour's share stays in this cell's slots until
-                        // the move that follows the step (launch_nee_move); the
-                        // neighbour's (rho, j / rho) from the record (zero
-                        // acceleration: u = j / (rho (1 + alpha / 2)))
-                        const uint32_t xn = (uint32_t)((int64_t)x + pm.nb_off);
-                        const float sc = 1.f + 0.5f * a.alpha[xn];
-                        const float un[3] = {a.record[(size_t)n + xn] * sc, a.record[2 * (size_t)n + xn] * sc,
-                                             a.record[3 * (size_t)n + xn] * sc};
-                        nee_transpose<Q>(pm, a.record[xn], un, v);
+                        // nonlinear ports, linearised at the recorded (rho, j / rho)
+                        // of port_lin_cell (zero acceleration: u = j / (rho (1 +
+                        // alpha / 2))); an extrapolating port's share for its
+                        // neighbour stays in this cell's slots until the move that
+                        // follows the step (launch_nee_move)
+                        const size_t xm = (size_t)port_lin_cell(pm, x);
+                        const float sc = 1.f + 0.5f * a.alpha[xm];
+                        const float um[3] = {a.record[(size_t)n + xm] * sc, a.record[2 * (size_t)n + xm] * sc,
+                                             a.record[3 * (size_t)n + xm] * sc};
+                        port_vjp<Q>(pm, a.record[xm], um, v);
                     }
                 }
                 store_own_lam<Q, T>(D, n, x, v, k_out);

@@ -109,6 +109,10 @@ struct PortMap {
     int32_t rb_nb, ub_nb;
     float rb1;
     float u_port[3];
+    // regularized known-stress port (recon 3): the least-squares stress fit
+    // over the known populations, stress[r] = sum_q sop[r][q] (f_q - eq_q)
+    // (zero columns for the unknown populations)
+    float sop[6][27];
 };
 
 // ------------------------------------------------------------------ arguments

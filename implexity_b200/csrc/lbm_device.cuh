@@ -371,16 +371,139 @@ __device__ __forceinline__ void nee_transpose(const PortMap& P, float rp_n, cons
     for (int q = 0; q < Q; ++q) v[q] += rnb + L::cx(q) * jb[0] + L::cy(q) * jb[1] + L::cz(q) * jb[2];
 }
 
+// ------------------------------------------------------------------ regularized port
+// Regularized known-stress port (ports.rs reconstruct_regularized :455-482):
+// the legacy target fixes (rho, u); every population is replaced by
+// eq(rho, u) + sum_r stress_r B_qr, with the deviatoric basis B_qr = 4.5 w_q
+// (c_a c_b - delta_ab / 3) over (xx, yy, zz, 2xy, 2xz, 2yz) and the stress
+// fitted to the known populations' non-equilibrium parts.
+template <int Q>
+__device__ __forceinline__ constexpr float stress_basis(int q, int r) {
+    using L = Lat<Q>;
+    const int c[3] = {L::cx(q), L::cy(q), L::cz(q)};
+    const int ia = r < 3 ? r : (r == 5 ? 1 : 0);
+    const int ib = r < 3 ? r : (r == 3 ? 1 : 2);
+    const float qq = (float)(c[ia] * c[ib]) - (ia == ib ? 1.f / 3.f : 0.f);
+    return 4.5f * L::w(q) * (r < 3 ? qq : 2.f * qq);
+}
+
+template <int Q>
+__device__ __forceinline__ void regularized_apply(const PortMap& P, float (&g)[Q]) {
+    using L = Lat<Q>;
+    float t[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) t[q] = g[q];
+    apply_port<Q>(P, t);
+    float rp, u[3];
+    nee_moments<Q, float>(t, rp, u);
+    const float rho = 1.f + rp, u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    // e = eq - w in shifted variables
+    float st[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const float cu = L::cx(q) * u[0] + L::cy(q) * u[1] + L::cz(q) * u[2];
+        t[q] = L::w(q) * (rp + rho * (3.f * cu + 4.5f * cu * cu - 1.5f * u2));
+        const float ne = g[q] - t[q];
+#pragma unroll
+        for (int r = 0; r < 6; ++r) st[r] = fmaf(P.sop[r][q], ne, st[r]);
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        float acc = t[q];
+#pragma unroll
+        for (int r = 0; r < 6; ++r) acc = fmaf(st[r], stress_basis<Q>(q, r), acc);
+        g[q] = acc;
+    }
+}
+
+// v <- the cotangent of the streamed populations given v, the cotangent of
+// the rebuilt ones, at the rebuilt cell's (rho - 1, u): the map is nonlinear
+// only through the legacy target's density and velocity, which the rebuilt
+// cell carries unchanged (the stress basis has no mass or momentum).
+template <int Q>
+__device__ __forceinline__ void regularized_transpose(const PortMap& P, float rp, const float (&u)[3], float (&v)[Q]) {
+    using L = Lat<Q>;
+    float sb[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+#pragma unroll
+        for (int r = 0; r < 6; ++r) sb[r] = fmaf(v[q], stress_basis<Q>(q, r), sb[r]);
+    const float rho = 1.f + rp, u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    float rb = 0.f, ub[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        float d = 0.f;
+#pragma unroll
+        for (int r = 0; r < 6; ++r) d = fmaf(sb[r], P.sop[r][q], d);
+        // the stress reads the known populations directly (d) and the
+        // equilibrium through -d
+        const float eb = (v[q] - d) * L::w(q);
+        v[q] = d;
+        const float cu = L::cx(q) * u[0] + L::cy(q) * u[1] + L::cz(q) * u[2];
+        rb += eb * (1.f + 3.f * cu + 4.5f * cu * cu - 1.5f * u2);
+        const float c[3] = {(float)L::cx(q), (float)L::cy(q), (float)L::cz(q)};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) ub[k] += eb * rho * (3.f * c[k] + 9.f * cu * c[k] - 3.f * u[k]);
+    }
+    const float inv = 1.f / rho;
+    float jb[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        jb[k] = ub[k] * inv;
+        rb -= ub[k] * u[k] * inv;
+    }
+    // through the legacy target (affine; its transpose is port_transpose)
+    float tb[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) tb[q] = rb + L::cx(q) * jb[0] + L::cy(q) * jb[1] + L::cz(q) * jb[2];
+    port_transpose<Q>(P, tb);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) v[q] += tb[q];
+}
+
+// Transposed port map of one port cell, in place on v.  rp / u: the density
+// - 1 and velocity j / rho of the cell the map is linearised at (the inward
+// neighbour for the extrapolations, the rebuilt cell itself for the
+// regularized port; unused by the affine legacy map).
+template <int Q>
+__device__ __forceinline__ void port_vjp(const PortMap& P, float rp, const float (&u)[3], float (&v)[Q]) {
+    if (P.recon == 3) regularized_transpose<Q>(P, rp, u, v);
+    else if (P.recon) nee_transpose<Q>(P, rp, u, v);
+    else port_transpose<Q>(P, v);
+}
+
+// The cell whose (rho, u) a port cell's transpose is linearised at.
+__device__ __forceinline__ int64_t port_lin_cell(const PortMap& P, int64_t x) {
+    return (P.recon == 1 || P.recon == 2) ? x + P.nb_off : x;
+}
+
 // The post-port populations g of port cell x (shifted) from the population
-// array A: the legacy affine map on its own streamed g, or the extrapolation
-// from the inward neighbour's streamed populations (read through the same
-// pull).  Returns the exchanged mass; rp_n / u_n receive the neighbour's
-// (rho - 1, j / rho) for the extrapolating ports.
+// array A: the legacy affine map on its own streamed g, the regularized
+// port, or the extrapolation from the inward neighbour's streamed
+// populations (read through the same pull).  Returns the exchanged mass;
+// rp_n / u_n receive the (rho - 1, j / rho) the transpose is linearised at
+// (port_lin_cell's) for the nonlinear ports.
 template <int Q, typename T>
 __device__ __forceinline__ float port_state(const PortMap& P, const T* __restrict__ A, const Geometry& G,
                                             const uint32_t* __restrict__ mask, uint32_t x, float (&g)[Q],
                                             float* rp_n = nullptr, float* u_n = nullptr) {
     if (!P.recon) return apply_port<Q>(P, g);
+    if (P.recon == 3) {
+        float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) s0 += g[q];
+        regularized_apply<Q>(P, g);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) s1 += g[q];
+        if (rp_n) {
+            float u[3];
+            nee_moments<Q, float>(g, *rp_n, u);
+            u_n[0] = u[0];
+            u_n[1] = u[1];
+            u_n[2] = u[2];
+        }
+        return s1 - s0;
+    }
     const uint32_t xn = (uint32_t)((int64_t)x + P.nb_off);
     float gn[Q], out[Q];
     load_pop<Q, T>(A, G, xn, mask[xn], gn);

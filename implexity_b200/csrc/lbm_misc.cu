@@ -67,7 +67,14 @@ __global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
             double gd[Q];
 #pragma unroll
             for (int q = 0; q < Q; ++q) gd[q] = g[q];
-            if (a.apply_ports && pm && pm->recon) {
+            if (a.apply_ports && pm && pm->recon == 3) {
+                float gp[Q];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) gp[q] = g[q];
+                regularized_apply<Q>(*pm, gp);
+#pragma unroll
+                for (int q = 0; q < Q; ++q) gd[q] = gp[q];
+            } else if (a.apply_ports && pm && pm->recon) {
                 // extrapolation from the inward neighbour's streamed populations
                 const uint32_t xn = (uint32_t)((int64_t)x + pm->nb_off);
                 float gnf[Q];
@@ -139,7 +146,7 @@ __global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
             }
             continue;
         }
-        // the neighbour's (rho - 1, j / rho) of an extrapolating port cell
+        // the (rho - 1, j / rho) a nonlinear port's transpose is linearised at
         float rpn = 0.f, un[3] = {0.f, 0.f, 0.f};
         if (pm && pm->recon && (a.apply_ports || a.port_transpose)) {
             float gp[Q];
@@ -177,10 +184,7 @@ __global__ void __launch_bounds__(BLOCK) k_objective(ObjArgs a) {
             }
             // (an extrapolating port cell keeps its neighbour's share in its own
             // slots for launch_nee_move)
-            if (a.port_transpose && pm) {
-                if (pm->recon) nee_transpose<Q>(*pm, rpn, un, fb);
-                else port_transpose<Q>(*pm, fb);
-            }
+            if (a.port_transpose && pm) port_vjp<Q>(*pm, rpn, un, fb);
             if (a.write_lambda) {
                 TL* B = static_cast<TL*>(a.lam);
 #pragma unroll
@@ -253,9 +257,9 @@ __global__ void __launch_bounds__(BLOCK) k_canon_lam(Geometry G, const T* B, con
 }
 
 // Natural lambda (cotangent of the post-port state) -> stored seed layout.
-// Extrapolating port cells take the neighbour's (rho - 1, u) from rec_next,
-// the record of the state lambda belongs to, and keep the neighbour's share
-// in their own slots for launch_nee_move.
+// Nonlinear port cells take the (rho - 1, u) they are linearised at from
+// rec_next, the record of the state lambda belongs to; extrapolating ones
+// keep the neighbour's share in their own slots for launch_nee_move.
 template <int Q, typename T>
 __global__ void __launch_bounds__(BLOCK) k_seed_lam(Geometry G, T* B, const uint32_t* __restrict__ mask,
                                                     const PortMap* ports, const float* in, float scale,
@@ -272,10 +276,10 @@ __global__ void __launch_bounds__(BLOCK) k_seed_lam(Geometry G, T* B, const uint
             if (!pm.recon) {
                 port_transpose<Q>(pm, v);
             } else {
-                const int64_t xn = x + pm.nb_off;
-                const float sc = 1.f + 0.5f * alpha[xn];
-                const float un[3] = {rec_next[G.n + xn] * sc, rec_next[2 * G.n + xn] * sc, rec_next[3 * G.n + xn] * sc};
-                nee_transpose<Q>(pm, rec_next[xn], un, v);
+                const int64_t xm = port_lin_cell(pm, x);
+                const float sc = 1.f + 0.5f * alpha[xm];
+                const float um[3] = {rec_next[G.n + xm] * sc, rec_next[2 * G.n + xm] * sc, rec_next[3 * G.n + xm] * sc};
+                port_vjp<Q>(pm, rec_next[xm], um, v);
             }
         }
 #pragma unroll

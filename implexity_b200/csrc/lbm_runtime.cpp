@@ -174,7 +174,54 @@ struct PortSpec {
     double freq = 0, phase = 0, ramp = 0;
     int recon = LBM_RECON_LEGACY_MOMENT;  // lbm_port_reconstruction
     int64_t nb_off = 0;                   // inward neighbour offset (extrapolating ports)
+    double sop[6][27] = {};               // regularized port: the known-stress fit
 };
+
+// The regularized port's stress fit (ports.rs known_stress_operator
+// :409-439): the weighted least-squares inverse of the deviatoric basis
+// B_qr = 4.5 w_q (c_a c_b - delta_ab / 3) over the known populations
+// (c_axis != sign), sop[r][q] = sum_c (M^T M)^-1_rc B_qc / w_q with
+// M_qc = B_qc / sqrt(w_q); zero for the unknown populations.  False when the
+// fit is rank deficient (a pivot below 1e-12 of the largest diagonal).
+double stress_basis_h(const HostLat& L, int q, int r) {
+    static const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+    const double qq = L.c[q][ia[r]] * L.c[q][ib[r]] - (ia[r] == ib[r] ? 1.0 / 3.0 : 0.0);
+    return 4.5 * L.w[q] * (r < 3 ? qq : 2.0 * qq);
+}
+
+bool regularized_fit(const HostLat& L, int axis, int sign, double (&sop)[6][27]) {
+    double A[6][12] = {};
+    for (int r = 0; r < 6; ++r) {
+        for (int c = 0; c < 6; ++c)
+            for (int q = 0; q < L.Q; ++q)
+                if (L.c[q][axis] != sign) A[r][c] += stress_basis_h(L, q, r) * stress_basis_h(L, q, c) / L.w[q];
+        A[r][6 + r] = 1.0;
+    }
+    double big = 0.0;
+    for (int r = 0; r < 6; ++r) big = std::max(big, std::fabs(A[r][r]));
+    for (int c = 0; c < 6; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < 6; ++r)
+            if (std::fabs(A[r][c]) > std::fabs(A[piv][c])) piv = r;
+        if (!(std::fabs(A[piv][c]) > 1e-12 * big)) return false;
+        for (int j = 0; j < 12; ++j) std::swap(A[c][j], A[piv][j]);
+        const double d = A[c][c];
+        for (int j = 0; j < 12; ++j) A[c][j] /= d;
+        for (int r = 0; r < 6; ++r) {
+            if (r == c) continue;
+            const double m = A[r][c];
+            for (int j = 0; j < 12; ++j) A[r][j] -= m * A[c][j];
+        }
+    }
+    for (int r = 0; r < 6; ++r)
+        for (int q = 0; q < 27; ++q) {
+            double acc = 0.0;
+            if (q < L.Q && L.c[q][axis] != sign)
+                for (int c = 0; c < 6; ++c) acc += A[r][6 + c] * stress_basis_h(L, q, c);
+            sop[r][q] = q < L.Q ? acc / L.w[q] : 0.0;
+        }
+    return true;
+}
 
 // Signal::factors (moving/boundary.rs:111-125): the C2 smoothstep ramp and
 // the sine wave at time t seconds.
@@ -375,6 +422,7 @@ struct lbm_handle {
     // port) per group; their transposes move cotangents to the neighbours
     std::vector<std::array<int64_t, 3>> nee_groups;
     DevBuf nee_cells_d;
+    bool nonlinear_ports = false;  // a port other than legacy_moment (transposes read a record)
     // --- state
     bool design_set = false, state_valid = false, forward_done = false;
     int cur = 0;   // which population array holds the current state
@@ -460,7 +508,10 @@ std::vector<PortMap> port_maps_at(const lbm_handle& h, double t_s) {
         // extrapolating ports: which of the boundary density / velocity the
         // neighbour supplies (ports.rs:484-497, moving/boundary.rs:445-458)
         M.recon = spec.recon;
-        if (spec.recon != LBM_RECON_LEGACY_MOMENT) {
+        if (spec.recon == LBM_RECON_REGULARIZED_KNOWN_STRESS)
+            for (int r = 0; r < 6; ++r)
+                for (int q = 0; q < 27; ++q) M.sop[r][q] = (float)spec.sop[r][q];
+        if (spec.recon == LBM_RECON_NEIGHBOR_NON_EQUILIBRIUM || spec.recon == LBM_RECON_NON_EQUILIBRIUM_EXTRAPOLATION) {
             M.nb_off = (int32_t)spec.nb_off;
             const bool neighbor = spec.recon == LBM_RECON_NEIGHBOR_NON_EQUILIBRIUM;
             M.rb_nb = (!neighbor && !spec.pressure) ? 1 : 0;
@@ -665,16 +716,23 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
             require(!(p.solid_mask[x] || p.design_region[x] || p.fixed_design[x] != 1.0),
                     "Port cells must be protected, unobstructed, fixed-design fluid");
         // reconstruction (ports.rs:134-157, 202-219)
-        require(pt.reconstruction >= LBM_RECON_LEGACY_MOMENT && pt.reconstruction <= LBM_RECON_NON_EQUILIBRIUM_EXTRAPOLATION,
-                "Port reconstruction must be legacy_moment, neighbor_non_equilibrium or non_equilibrium_extrapolation");
+        require(pt.reconstruction >= LBM_RECON_LEGACY_MOMENT && pt.reconstruction <= LBM_RECON_REGULARIZED_KNOWN_STRESS,
+                "Port reconstruction must be legacy_moment, regularized_known_stress, neighbor_non_equilibrium or "
+                "non_equilibrium_extrapolation");
         s.recon = pt.reconstruction;
         const bool accelerated = p.acceleration_m_s2[0] != 0.0 || p.acceleration_m_s2[1] != 0.0 ||
                                  p.acceleration_m_s2[2] != 0.0;
+        require(!(s.recon == LBM_RECON_REGULARIZED_KNOWN_STRESS && accelerated),
+                "regularized_known_stress ports require zero acceleration; forcing-consistent stress reconstruction is "
+                "not implemented");
         require(!(s.recon == LBM_RECON_NEIGHBOR_NON_EQUILIBRIUM && (!s.pressure || accelerated)),
                 "neighbor_non_equilibrium currently requires a pressure port and zero acceleration");
         require(!(s.recon == LBM_RECON_NON_EQUILIBRIUM_EXTRAPOLATION && accelerated),
                 "non_equilibrium_extrapolation requires zero acceleration");
-        if (s.recon != LBM_RECON_LEGACY_MOMENT) {
+        if (s.recon == LBM_RECON_REGULARIZED_KNOWN_STRESS)
+            require(regularized_fit(h.L, s.axis, s.sign, s.sop),
+                    "Regularized port stress fit is rank deficient or ill conditioned");
+        if (s.recon == LBM_RECON_NEIGHBOR_NON_EQUILIBRIUM || s.recon == LBM_RECON_NON_EQUILIBRIUM_EXTRAPOLATION) {
             require(shape[s.axis] >= 2, "Neighbor pressure reconstruction requires an inward fluid plane");
             const int64_t stride[3] = {h.G.sx, h.G.sy, 1};
             s.nb_off = s.sign * stride[s.axis];
@@ -728,8 +786,10 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
     h.n_ports = (int)specs.size();
     // an extrapolating port reads its neighbours' streamed populations, which
     // must not be rebuilt by a port themselves
+    h.nonlinear_ports = false;
+    for (size_t k = 0; k < specs.size(); ++k) h.nonlinear_ports = h.nonlinear_ports || specs[k].recon != 0;
     for (size_t k = 0; k < specs.size(); ++k)
-        if (specs[k].recon != LBM_RECON_LEGACY_MOMENT)
+        if (specs[k].recon == LBM_RECON_NEIGHBOR_NON_EQUILIBRIUM || specs[k].recon == LBM_RECON_NON_EQUILIBRIUM_EXTRAPOLATION)
             for (int64_t x : port_cells[k])
                 require(!used[x + specs[k].nb_off], "The inward neighbours of an extrapolating port cannot be port cells");
     h.n_inlet = h.n_outlet = 0;
@@ -774,7 +834,8 @@ void validate_and_build(lbm_handle& h, const lbm_problem_t& p) {
     std::vector<uint32_t> nee_cells;
     h.nee_groups.clear();
     for (size_t k = 0; k < port_cells.size(); ++k) {
-        if (specs[k].recon == LBM_RECON_LEGACY_MOMENT) continue;
+        if (specs[k].recon != LBM_RECON_NEIGHBOR_NON_EQUILIBRIUM && specs[k].recon != LBM_RECON_NON_EQUILIBRIUM_EXTRAPOLATION)
+            continue;
         h.nee_groups.push_back({(int64_t)nee_cells.size(), (int64_t)port_cells[k].size(), (int64_t)k});
         for (int64_t x : port_cells[k]) nee_cells.push_back((uint32_t)x);
     }
@@ -2212,11 +2273,12 @@ lbm_status step_vjp_impl(lbm_handle* h, const double* state, const double* lambd
     }
     alloc_adjoint(*h, LBM_STORE_F32);
     h->record.alloc(((size_t)N * 4 + CELL_PAD) * sizeof(float), ctr);
-    // extrapolating ports transpose at the neighbours of the next state:
-    // its (rho - 1, u) record from one step into the other array, which
-    // leaves the current one (this state) in place
+    // nonlinear ports transpose at the next state (the extrapolations at the
+    // neighbours, the regularized port at the port cell): its (rho - 1, u)
+    // record from one step into the other array, which leaves the current
+    // one (this state) in place
     DevBuf rec_next;
-    if (!h->nee_groups.empty()) {
+    if (h->nonlinear_ports) {
         rec_next.alloc(((size_t)N * 4 + CELL_PAD) * sizeof(float), ctr);
         const int cur = h->cur;
         const int64_t t0 = h->t;

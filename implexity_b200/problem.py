@@ -42,7 +42,12 @@ PROBLEM_KEYS = sorted(
     ]
 )
 # port reconstructions (ports.rs:134-147) and the moving engine's extrapolation (moving/boundary.rs:445-506)
-RECONSTRUCTIONS = {"legacy_moment": 0, "neighbor_non_equilibrium": 1, "non_equilibrium_extrapolation": 2}
+RECONSTRUCTIONS = {
+    "legacy_moment": 0,
+    "neighbor_non_equilibrium": 1,
+    "non_equilibrium_extrapolation": 2,
+    "regularized_known_stress": 3,
+}
 OPTIONAL_KEYS = ["topology_map", "ports", "origin_m", "field_registration", "geometry_source", "solver_options"]
 
 STORAGE = {"float32": _abi.LBM_STORE_F32, "float16": _abi.LBM_STORE_F16, "bfloat16": _abi.LBM_STORE_BF16}
@@ -278,9 +283,6 @@ def _ports(value: Any, shape: tuple[int, int, int]) -> list[dict]:
             raise _err(
                 "Port reconstruction must be legacy_moment, regularized_known_stress or neighbor_non_equilibrium"
             )
-        if rec == "regularized_known_stress":
-            raise _err("Port reconstruction regularized_known_stress is not provided by the GPU provider; use "
-                       "legacy_moment, neighbor_non_equilibrium or non_equilibrium_extrapolation")
         ids.add(pid)
         if port.get("face") not in _abi.FACES:
             raise _err("Port must identify one Cartesian face")

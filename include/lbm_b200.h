@@ -96,12 +96,18 @@ typedef enum { LBM_PORT_VELOCITY = 0, LBM_PORT_PRESSURE = 1 } lbm_port_kind;
  * NON_EQUILIBRIUM_EXTRAPOLATION: the moving engine's port (moving/boundary.rs:
  *   445-506), f = eq(rho_b, u_b) + f_n - eq(rho_n, u_n) with (rho_n, u_port) on
  *   velocity ports and (rho_port, u_n) on pressure ports.
- * Both extrapolations need zero acceleration (ports.rs:148-157); their
- * transposes add into the neighbour's cotangent after each transposed step. */
+ * REGULARIZED_KNOWN_STRESS: every population as eq(rho, u) of the legacy
+ *   target plus the deviatoric stress fitted to the known populations'
+ *   non-equilibrium parts (ports.rs reconstruct_regularized :409-482).
+ * The three need zero acceleration (ports.rs:148-157); the extrapolations'
+ * inward neighbours must be protected fluid cells that are not port cells
+ * (ports.rs:202-219), and their transposes add into the neighbour's
+ * cotangent after each transposed step. */
 typedef enum {
     LBM_RECON_LEGACY_MOMENT = 0,
     LBM_RECON_NEIGHBOR_NON_EQUILIBRIUM = 1,
-    LBM_RECON_NON_EQUILIBRIUM_EXTRAPOLATION = 2
+    LBM_RECON_NON_EQUILIBRIUM_EXTRAPOLATION = 2,
+    LBM_RECON_REGULARIZED_KNOWN_STRESS = 3
 } lbm_port_reconstruction;
 
 /* Faces in the order of ports.rs FACES: xmin, xmax, ymin, ymax, zmin, zmax. */
@@ -201,7 +207,7 @@ typedef struct {
      * only; no reference counterpart, the reference is FP64 throughout).
      * FP32 collision arithmetic rounds the equilibrium momentum coherently
      * over a nearly uniform flow, which biases the steady pressure by ~1e-7
-     * in density; FP64 collision removes that bias at ~1.6x the forward
+     * in density; FP64 collision removes that bias at ~1.8x the forward
      * step's time.  The adjoint is FP32 in both cases. */
     int32_t collision_fp64;
 } lbm_problem_t;

@@ -147,9 +147,11 @@ struct Port {
     int axis = 0, sign = 1;
     // 0: legacy moment (ports.rs:343-406); 1: neighbor_non_equilibrium
     // (ports.rs:484-497); 2: the moving engine's non-equilibrium extrapolation
-    // (moving/boundary.rs:445-460).  1 and 2 read the inward neighbour.
+    // (moving/boundary.rs:445-460); 3: regularized_known_stress
+    // (ports.rs:409-482).  1 and 2 read the inward neighbour.
     int recon = 0;
     int64_t nb_off = 0;
+    std::vector<double> sop;  // 3: the known-stress fit, 6 x Q (zero columns for the unknown populations)
     double vel[3] = {0, 0, 0};  // value in force at the current time
     double density = 1.0;
     std::vector<int64_t> cells;
@@ -444,6 +446,122 @@ void nee_vjp(const orc_problem& o, const Port& p, const double* nb, const double
         double v = g[q] + rn;
         for (int d = 0; d < 3; ++d) v += jb[d] * L.c[q][d];
         nb_bar[q] = v;
+    }
+}
+
+// Regularized known-stress port (ports.rs known_stress_operator :409-439,
+// reconstruct_regularized :455-482).  Basis of the deviatoric second
+// moment: B[q][r] = 4.5 w_q (c_a c_b - delta_ab / 3) over (xx, yy, zz, 2xy,
+// 2xz, 2yz).  The stress is the weighted least-squares fit of the known
+// populations' non-equilibrium parts (known: c_axis != sign), sop = pinv(M)
+// with M[k][r] = B[known_k][r] / sqrt(w), columns rescaled by 1 / sqrt(w).
+double stress_basis(const Lattice& L, int q, int r) {
+    static const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+    const double qq = L.c[q][ia[r]] * L.c[q][ib[r]] - (ia[r] == ib[r] ? 1.0 / 3.0 : 0.0);
+    return 4.5 * L.w[q] * (r < 3 ? qq : 2.0 * qq);
+}
+
+bool regularized_operator(const Lattice& L, Port& pt) {
+    const int Q = L.Q;
+    std::vector<int> known;
+    for (int q = 0; q < Q; ++q)
+        if (L.c[q][pt.axis] != pt.sign) known.push_back(q);
+    const int K = (int)known.size();
+    // pinv of the full-column-rank K x 6 matrix M: (M^T M)^-1 M^T
+    double G[6][12] = {};
+    for (int r = 0; r < 6; ++r) {
+        for (int c2 = 0; c2 < 6; ++c2) {
+            double acc = 0;
+            for (int k = 0; k < K; ++k) {
+                const double wq = L.w[known[k]];
+                acc += stress_basis(L, known[k], r) * stress_basis(L, known[k], c2) / wq;
+            }
+            G[r][c2] = acc;
+        }
+        G[r][6 + r] = 1.0;
+    }
+    double scale = 0;
+    for (int r = 0; r < 6; ++r) scale = std::max(scale, std::fabs(G[r][r]));
+    for (int c2 = 0; c2 < 6; ++c2) {
+        int piv = c2;
+        for (int r = c2 + 1; r < 6; ++r)
+            if (std::fabs(G[r][c2]) > std::fabs(G[piv][c2])) piv = r;
+        if (std::fabs(G[piv][c2]) <= 1e-12 * scale) return false;  // rank deficient
+        for (int j = 0; j < 12; ++j) std::swap(G[c2][j], G[piv][j]);
+        const double d = G[c2][c2];
+        for (int j = 0; j < 12; ++j) G[c2][j] /= d;
+        for (int r = 0; r < 6; ++r) {
+            if (r == c2) continue;
+            const double m = G[r][c2];
+            for (int j = 0; j < 12; ++j) G[r][j] -= m * G[c2][j];
+        }
+    }
+    // sop[r][q] = sum_c inv[r][c] M[k][c] / sqrt(w) = sum_c inv[r][c] B[q][c] / w
+    pt.sop.assign((size_t)6 * Q, 0.0);
+    for (int r = 0; r < 6; ++r)
+        for (int q : known) {
+            double acc = 0;
+            for (int c2 = 0; c2 < 6; ++c2) acc += G[r][6 + c2] * stress_basis(L, q, c2);
+            pt.sop[(size_t)r * Q + q] = acc / L.w[q];
+        }
+    return true;
+}
+
+void regularized_apply(const orc_problem& o, const Port& p, const double* f, double* out) {
+    const Lattice& L = o.L;
+    const int Q = L.Q;
+    double tgt[27], rho, j[3], u[3], eq[27], stress[6] = {0, 0, 0, 0, 0, 0};
+    reconstruct(o, p, f, tgt);
+    moments(L, tgt, rho, j);
+    for (int d = 0; d < 3; ++d) u[d] = j[d] / rho;
+    const double u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    for (int q = 0; q < Q; ++q) {
+        const double cu = dotc(L, q, u);
+        eq[q] = rho * L.w[q] * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * u2);
+    }
+    for (int r = 0; r < 6; ++r)
+        for (int q = 0; q < Q; ++q) stress[r] += (f[q] - eq[q]) * p.sop[(size_t)r * Q + q];
+    for (int q = 0; q < Q; ++q) {
+        double acc = eq[q];
+        for (int r = 0; r < 6; ++r) acc += stress[r] * stress_basis(L, q, r);
+        out[q] = acc;
+    }
+}
+
+// Transpose of regularized_apply at a streamed state whose rebuilt
+// populations are `post`: the map depends on the streamed populations
+// nonlinearly only through the density and velocity of the legacy target,
+// and the rebuilt cell carries exactly those (the stress basis has no mass
+// or momentum), so post's moments fix the linearisation.
+void regularized_vjp(const orc_problem& o, const Port& p, const double* post, const double* g, double* fb) {
+    const Lattice& L = o.L;
+    const int Q = L.Q;
+    double rho, j[3], u[3];
+    moments(L, post, rho, j);
+    for (int d = 0; d < 3; ++d) u[d] = j[d] / rho;
+    double sb[6] = {0, 0, 0, 0, 0, 0}, direct[27], eqb[27];
+    for (int r = 0; r < 6; ++r)
+        for (int q = 0; q < Q; ++q) sb[r] += g[q] * stress_basis(L, q, r);
+    for (int q = 0; q < Q; ++q) {
+        double acc = 0;
+        for (int r = 0; r < 6; ++r) acc += sb[r] * p.sop[(size_t)r * Q + q];
+        direct[q] = acc;
+        eqb[q] = g[q] - acc;
+    }
+    double rb = 0, ub[3] = {0, 0, 0};
+    eq_vjp(o, rho, u, eqb, 1.0, rb, ub);
+    double jb[3];
+    for (int d = 0; d < 3; ++d) {
+        jb[d] = ub[d] / rho;
+        rb -= ub[d] * u[d] / rho;
+    }
+    double tb[27];
+    for (int q = 0; q < Q; ++q) tb[q] = rb + jb[0] * L.c[q][0] + jb[1] * L.c[q][1] + jb[2] * L.c[q][2];
+    // the legacy target is affine: its Jacobian p.jac (rows r, columns k)
+    for (int k = 0; k < Q; ++k) {
+        double acc = direct[k];
+        for (int r = 0; r < Q; ++r) acc += p.jac[(size_t)r * Q + k] * tb[r];
+        fb[k] = acc;
     }
 }
 
@@ -848,7 +966,8 @@ double interval(const orc_problem& o, const double* before, const double* alpha,
     for (const Port& p : o.ports) {
         for (int64_t cell : p.cells) {
             double vals[27];
-            if (p.recon) nee_apply(o, p, after + (cell + p.nb_off) * Q, vals);
+            if (p.recon == 3) regularized_apply(o, p, after + cell * Q, vals);
+            else if (p.recon) nee_apply(o, p, after + (cell + p.nb_off) * Q, vals);
             else reconstruct(o, p, after + cell * Q, vals);
             for (int q = 0; q < Q; ++q) {
                 exch += vals[q] - after[cell * Q + q];
@@ -884,6 +1003,12 @@ void interval_vjp(const orc_problem& o, const double* before, const double* alph
             bool any = false;
             for (int r = 0; r < Q; ++r) any |= g[r] != 0.0;
             if (!any) continue;
+            if (p.recon == 3) {
+                double fb[27];
+                regularized_vjp(o, p, streamed.data() + cell * Q, g, fb);
+                for (int k = 0; k < Q; ++k) refl[cell * Q + k] += fb[k];
+                continue;
+            }
             if (p.recon) {
                 double nb_bar[27];
                 nee_vjp(o, p, streamed.data() + (cell + p.nb_off) * Q, g, nb_bar);
@@ -1328,6 +1453,11 @@ int orc_create(const lbm_problem_t* p, orc_problem** out) {
         const int64_t stride[3] = {o->shape[1] * o->shape[2], o->shape[2], 1};
         pt.nb_off = pt.sign * stride[pt.axis];
         port_jacobian(*o, pt);
+        if (pt.recon == 3 && !regularized_operator(o->L, pt)) {
+            g_error = "Regularized port stress fit is rank deficient or ill conditioned";
+            delete o;
+            return 1;
+        }
         for (int64_t x : pt.cells) o->port_role[x] = pt.pressure ? -1 : 1;
         if (pt.pressure) o->n_outlet += (int64_t)pt.cells.size();
         else o->n_inlet += (int64_t)pt.cells.size();
@@ -1592,7 +1722,8 @@ int64_t orc_wall_loads(const orc_problem* o, const double* before, const double*
 
 void orc_port_apply(const orc_problem* o, int port, const double* f_in, double* f_out) {
     // the extrapolating reconstructions read the inward neighbour's populations
-    if (o->ports[port].recon) nee_apply(*o, o->ports[port], f_in, f_out);
+    if (o->ports[port].recon == 3) regularized_apply(*o, o->ports[port], f_in, f_out);
+    else if (o->ports[port].recon) nee_apply(*o, o->ports[port], f_in, f_out);
     else reconstruct(*o, o->ports[port], f_in, f_out);
 }
 

@@ -1,6 +1,9 @@
-"""Ports that rebuild their cells from the inward neighbour: ports.rs's
-neighbor_non_equilibrium (:484-497) and the moving engine's non-equilibrium
-extrapolation (moving/boundary.rs:445-506, port_populations and its VJP).
+"""The nonlinear port reconstructions: the two that rebuild a port cell from
+its inward neighbour, ports.rs's neighbor_non_equilibrium (:484-497) and the
+moving engine's non-equilibrium extrapolation (moving/boundary.rs:445-506,
+port_populations and its VJP), and ports.rs's regularized_known_stress
+(:409-482), which rebuilds every population from the cell's own legacy
+target and a stress fitted to its known populations.
 
 CPU: the oracle's transposed interval with these ports against FP64 central
 differences of one interval (directional, on the state).
@@ -29,6 +32,10 @@ def nee_channel(inlet, outlet, lattice="D3Q19", shape=(14, 8, 7), steps=120, col
                                      storage=storage, u_in=0.04)
     prob["ports"][0]["reconstruction"] = inlet
     prob["ports"][1]["reconstruction"] = outlet
+    # the extrapolations read protected, fixed-design inward planes (ports.rs:202-219)
+    design = np.asarray(prob["design_region"], bool).copy()
+    design[1] = design[-2] = False
+    prob["design_region"] = design
     return prob
 
 
@@ -36,6 +43,8 @@ CASES = [
     ("legacy_moment", "neighbor_non_equilibrium", "D3Q19"),
     ("non_equilibrium_extrapolation", "non_equilibrium_extrapolation", "D3Q19"),
     ("non_equilibrium_extrapolation", "neighbor_non_equilibrium", "D3Q27"),
+    ("regularized_known_stress", "regularized_known_stress", "D3Q19"),
+    ("regularized_known_stress", "neighbor_non_equilibrium", "D3Q27"),
 ]
 
 
@@ -72,6 +81,40 @@ def test_extrapolations_need_zero_acceleration_and_a_pressure_port():
     prob["acceleration_m_s2"] = [1e-6, 0.0, 0.0]
     with pytest.raises(ContractError, match="zero acceleration"):
         _create(prob)
+    prob = nee_channel("regularized_known_stress", "legacy_moment")
+    prob["acceleration_m_s2"] = [0.0, 1e-6, 0.0]
+    with pytest.raises(ContractError, match="regularized_known_stress ports require zero acceleration"):
+        _create(prob)
+    # the inward plane must be protected fluid
+    prob = nee_channel("legacy_moment", "neighbor_non_equilibrium")
+    design = np.asarray(prob["design_region"], bool).copy()
+    design[-2, 3, 3] = True
+    prob["design_region"] = design
+    with pytest.raises(ContractError, match="protected, unobstructed, fixed-design inward fluid cells"):
+        _create(prob)
+
+
+def test_regularized_port_keeps_the_legacy_density_and_velocity():
+    """The rebuilt cell carries the legacy target's density and momentum: the
+    stress basis has neither (the fact the transposed port relies on)."""
+    norm = normalize(nee_channel("regularized_known_stress", "regularized_known_stress", steps=10))
+    o = Oracle(norm)
+    _, alpha = o.design(workloads.uniform_design(norm.shape, 2))
+    f, _ = o.history(alpha, 10)
+    norm_l = normalize(nee_channel("legacy_moment", "legacy_moment", steps=10))
+    ol = Oracle(norm_l)
+    rng = np.random.default_rng(3)
+    cells = np.flatnonzero(np.asarray(norm.ports[0]["mask"]).reshape(-1))
+    for x in rng.choice(cells, 4, replace=False):
+        src = f[x] + 1e-3 * rng.standard_normal(f.shape[1])
+        reg = o.port_apply(0, src)
+        leg = ol.port_apply(0, src)
+        c = np.array([[0, 0, 0], [-1, -1, 0], [-1, 0, -1], [-1, 0, 0], [-1, 0, 1], [-1, 1, 0], [0, -1, -1],
+                      [0, -1, 0], [0, -1, 1], [0, 0, -1], [0, 0, 1], [0, 1, -1], [0, 1, 0], [0, 1, 1], [1, -1, 0],
+                      [1, 0, -1], [1, 0, 0], [1, 0, 1], [1, 1, 0]], float)
+        np.testing.assert_allclose(reg.sum(), leg.sum(), rtol=1e-13)
+        np.testing.assert_allclose(reg @ c, leg @ c, atol=1e-14)
+        assert np.max(np.abs(reg - leg)) > 1e-6  # the known populations are rebuilt too
 
 
 def _create(prob):
