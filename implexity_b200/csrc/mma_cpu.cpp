@@ -80,6 +80,11 @@ struct mma_handle {
     double ip_last_residual = 0.0;
     int64_t newton_steps = 0;
     std::string err;
+    // --- GCMMA (MmaOptimizer::gcmma, mma.rs:339-355; GcmmaState :242-248)
+    bool gcmma = false;
+    mma_gcmma_options_t g{};
+    int64_t nonfinite_trials = 0;
+    Vec rho_last;  // rho0 then rho of the last step
 
     // --- subproblem data (Sub, mma.rs:180-188)
     Vec p0, q0, P, Q, alpha, beta, b;
@@ -529,95 +534,248 @@ double mma_kkt_residual(const mma_handle* h, const double* x, const double* df0d
                                h->x_max.data());
 }
 
+// coerce (mma.rs:478-520), the KKT residual of the incoming iterate,
+// asymptote_update (:522-553) and trust_box (:555-571): the part of a step
+// before the subproblem's coefficients.  Returns the coerced iterate.
+static Vec begin_step(mma_handle* h, const double* x_k, const double* x_km1, const double* x_km2, double f0,
+                      const double* df0dx, const double* fs, const double* dfsdx, const double* x_new) {
+    const int64_t n = h->n, m = h->m;
+    if (!x_k || !x_km1 || !x_km2 || !df0dx || !x_new || (m > 0 && (!fs || !dfsdx)))
+        throw ContractError("MMA: input shapes must be x:(N,), df0dx:(N,), fs:(m,), dfsdx:(m,N) with N=" +
+                            std::to_string(n) + ", m=" + std::to_string(m) + ": cannot reshape");
+    const struct {
+        const char* name;
+        const double* v;
+        size_t len;
+    } arrs[] = {{"x_k", x_k, (size_t)n},      {"x_km1", x_km1, (size_t)n}, {"x_km2", x_km2, (size_t)n},
+                {"df0dx", df0dx, (size_t)n},  {"fs", fs, (size_t)m},       {"dfsdx", dfsdx, (size_t)(m * n)}};
+    for (const auto& a : arrs)
+        if (a.len && !all_finite(a.v, a.len)) throw ContractError(std::string("MMA: non-finite entries in ") + a.name);
+    if (!std::isfinite(f0)) throw ContractError("MMA: objective value f0 is not finite");
+    Vec xk(n);
+    bool inside = true;
+#pragma omp parallel for reduction(&& : inside) schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        inside = inside && x_k[i] >= h->x_min[i] - 1e-12 && x_k[i] <= h->x_max[i] + 1e-12;
+        xk[i] = std::min(std::max(x_k[i], h->x_min[i]), h->x_max[i]);
+    }
+    if (!inside) throw ContractError("MMA: x_k lies outside [x_min, x_max]");
+    h->last_kkt = mma_kkt_residual(h, xk.data(), df0dx, fs, dfsdx);
+    h->asymptote_update(xk.data(), x_km1, x_km2);
+    h->alpha.resize(n);
+    h->beta.resize(n);
+    const mma_options_t& o = h->o;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        const double l = h->low[i], u = h->upp[i], x = xk[i];
+        const double span = h->x_max[i] - h->x_min[i];
+        h->alpha[i] = std::max(std::max(l + o.albefa * (x - l), x - o.move_limit * span), h->x_min[i]);
+        h->beta[i] = std::min(std::min(u - o.albefa * (u - x), x + o.move_limit * span), h->x_max[i]);
+    }
+    return xk;
+}
+
+// pq / big_pq (mma.rs:573-615) with the objective's rho0 and the
+// constraints' rho (raa0 for every one in a plain step), and rhs (:617-622).
+static void build_sub(mma_handle* h, const Vec& xk, const double* df0dx, const double* fs, const double* dfsdx,
+                      double rho0, const Vec& rho) {
+    const int64_t n = h->n, m = h->m;
+    h->p0.resize(n);
+    h->q0.resize(n);
+    h->P.resize((size_t)m * n);
+    h->Q.resize((size_t)m * n);
+    Vec bsum(m, 0.0);
+#pragma omp parallel
+    {
+        Vec lb(m, 0.0);
+#pragma omp for schedule(static) nowait
+        for (int64_t i = 0; i < n; ++i) {
+            const double l = h->low[i], u = h->upp[i], x = xk[i];
+            const double ux2 = (u - x) * (u - x), xl2 = (x - l) * (x - l);
+            auto pq = [&](double df, double r, double& p, double& q) {
+                const double dfp = std::max(df, 0.0), dfm = std::max(-df, 0.0);
+                const double t = 0.001 * (dfp + dfm) + r / h->xmami[i];
+                p = (dfp + t) * ux2;
+                q = (dfm + t) * xl2;
+            };
+            pq(df0dx[i], rho0, h->p0[i], h->q0[i]);
+            for (int64_t j = 0; j < m; ++j) {
+                double& p = h->P[(size_t)j * n + i];
+                double& q = h->Q[(size_t)j * n + i];
+                pq(dfsdx[(size_t)j * n + i], rho[j], p, q);
+                lb[j] += p / (u - x) + q / (x - l);
+            }
+        }
+#pragma omp critical
+        for (int64_t j = 0; j < m; ++j) bsum[j] += lb[j];
+    }
+    h->b.resize(m);
+    for (int64_t j = 0; j < m; ++j) h->b[j] = bsum[j] - fs[j];
+}
+
+// record (mma.rs:771-797) and the step's diagnostics.
+static void finish_step(mma_handle* h, double* x_new, mma_info_t* info, std::chrono::steady_clock::time_point t0,
+                        int64_t inner, bool conservative) {
+    const double skkt = h->sub_kkt();
+    h->z = h->zv;
+    ++h->iter;
+    std::memcpy(x_new, h->x.data(), h->n * sizeof(double));
+    if (info) {
+        info->iteration = h->iter;
+        info->kkt_residual = h->last_kkt;
+        info->subproblem_kkt = skkt;
+        info->subproblem_converged = h->ip_converged ? 1 : 0;
+        info->subproblem_ip_residual = h->ip_last_residual;
+        info->z = h->z;
+        info->newton_steps = h->newton_steps;
+        info->wallclock_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        info->inner_iterations = inner;
+        info->conservative = conservative ? 1 : 0;
+    }
+}
+
 mma_status mma_step(mma_handle* h, const double* x_k, const double* x_km1, const double* x_km2, double f0,
                     const double* df0dx, const double* fs, const double* dfsdx, double* x_new, mma_info_t* info) {
     if (!h) return fail(nullptr, MMA_E_CONTRACT, "MMA: handle is NULL");
     const auto t0 = std::chrono::steady_clock::now();
     try {
-        const int64_t n = h->n, m = h->m;
-        if (!x_k || !x_km1 || !x_km2 || !df0dx || !x_new || (m > 0 && (!fs || !dfsdx)))
-            throw ContractError("MMA: input shapes must be x:(N,), df0dx:(N,), fs:(m,), dfsdx:(m,N) with N=" +
-                                std::to_string(n) + ", m=" + std::to_string(m) + ": cannot reshape");
-        // coerce (mma.rs:478-520)
-        const struct {
-            const char* name;
-            const double* v;
-            size_t len;
-        } arrs[] = {{"x_k", x_k, (size_t)n},      {"x_km1", x_km1, (size_t)n}, {"x_km2", x_km2, (size_t)n},
-                    {"df0dx", df0dx, (size_t)n},  {"fs", fs, (size_t)m},       {"dfsdx", dfsdx, (size_t)(m * n)}};
-        for (const auto& a : arrs)
-            if (a.len && !all_finite(a.v, a.len)) throw ContractError(std::string("MMA: non-finite entries in ") + a.name);
-        if (!std::isfinite(f0)) throw ContractError("MMA: objective value f0 is not finite");
-        Vec xk(n);
-        bool inside = true;
-#pragma omp parallel for reduction(&& : inside) schedule(static)
-        for (int64_t i = 0; i < n; ++i) {
-            inside = inside && x_k[i] >= h->x_min[i] - 1e-12 && x_k[i] <= h->x_max[i] + 1e-12;
-            xk[i] = std::min(std::max(x_k[i], h->x_min[i]), h->x_max[i]);
-        }
-        if (!inside) throw ContractError("MMA: x_k lies outside [x_min, x_max]");
-        h->last_kkt = mma_kkt_residual(h, xk.data(), df0dx, fs, dfsdx);
-        h->asymptote_update(xk.data(), x_km1, x_km2);
-        // trust_box (mma.rs:555-571), pq / big_pq (:573-615), rhs (:617-622)
-        h->alpha.resize(n);
-        h->beta.resize(n);
-        h->p0.resize(n);
-        h->q0.resize(n);
-        h->P.resize((size_t)m * n);
-        h->Q.resize((size_t)m * n);
-        Vec bsum(m, 0.0);
-        const mma_options_t& o = h->o;
-#pragma omp parallel
-        {
-            Vec lb(m, 0.0);
-#pragma omp for schedule(static) nowait
-            for (int64_t i = 0; i < n; ++i) {
-                const double l = h->low[i], u = h->upp[i], x = xk[i];
-                const double span = h->x_max[i] - h->x_min[i];
-                h->alpha[i] = std::max(std::max(l + o.albefa * (x - l), x - o.move_limit * span), h->x_min[i]);
-                h->beta[i] = std::min(std::min(u - o.albefa * (u - x), x + o.move_limit * span), h->x_max[i]);
-                const double ux2 = (u - x) * (u - x), xl2 = (x - l) * (x - l);
-                auto pq = [&](double df, double& p, double& q) {
-                    const double dfp = std::max(df, 0.0), dfm = std::max(-df, 0.0);
-                    const double t = 0.001 * (dfp + dfm) + o.raa0 / h->xmami[i];
-                    p = (dfp + t) * ux2;
-                    q = (dfm + t) * xl2;
-                };
-                pq(df0dx[i], h->p0[i], h->q0[i]);
-                for (int64_t j = 0; j < m; ++j) {
-                    double& p = h->P[(size_t)j * n + i];
-                    double& q = h->Q[(size_t)j * n + i];
-                    pq(dfsdx[(size_t)j * n + i], p, q);
-                    lb[j] += p / (u - x) + q / (x - l);
-                }
-            }
-#pragma omp critical
-            for (int64_t j = 0; j < m; ++j) bsum[j] += lb[j];
-        }
-        h->b.resize(m);
-        for (int64_t j = 0; j < m; ++j) h->b[j] = bsum[j] - fs[j];
+        if (h->gcmma)
+            throw ContractError("GCMMA.step requires eval_true(x) -> (f0, fs) to test conservativeness of the "
+                                "approximation at the trial point");
+        const Vec xk = begin_step(h, x_k, x_km1, x_km2, f0, df0dx, fs, dfsdx, x_new);
+        build_sub(h, xk, df0dx, fs, dfsdx, h->o.raa0, Vec(h->m, h->o.raa0));
         h->solve_subproblem();
-        const double skkt = h->sub_kkt();
-        // record (mma.rs:771-797)
-        h->z = h->zv;
-        ++h->iter;
-        std::memcpy(x_new, h->x.data(), n * sizeof(double));
-        if (info) {
-            info->iteration = h->iter;
-            info->kkt_residual = h->last_kkt;
-            info->subproblem_kkt = skkt;
-            info->subproblem_converged = h->ip_converged ? 1 : 0;
-            info->subproblem_ip_residual = h->ip_last_residual;
-            info->z = h->z;
-            info->newton_steps = h->newton_steps;
-            info->wallclock_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        }
+        finish_step(h, x_new, info, t0, 0, true);
         return MMA_OK;
     } catch (const ContractError& e) {
         return fail(h, MMA_E_CONTRACT, e.what());
     } catch (const std::exception& e) {
         return fail(h, MMA_E_RUNTIME, e.what());
     }
+}
+
+void mma_gcmma_default_options(mma_gcmma_options_t* g) {
+    if (!g) return;
+    g->rho_min = 1e-6;
+    g->rho_init = 0.1;
+    g->rho_growth = 10.0;
+    g->max_conservative = 15;
+}
+
+mma_status mma_enable_gcmma(mma_handle* h, const mma_gcmma_options_t* g) {
+    if (!h) return fail(nullptr, MMA_E_CONTRACT, "MMA: handle is NULL");
+    mma_gcmma_options_t o;
+    mma_gcmma_default_options(&o);
+    if (g) o = *g;
+    if (!(o.rho_min > 0.0 && o.rho_init > 0.0 && o.rho_growth > 1.0))
+        return fail(h, MMA_E_CONTRACT, "GCMMA: require rho_min > 0, rho_init > 0, rho_growth > 1");
+    if (o.max_conservative < 0) return fail(h, MMA_E_CONTRACT, "GCMMA: max_conservative must be >= 0");
+    h->gcmma = true;
+    h->g = o;
+    h->nonfinite_trials = 0;
+    h->rho_last.clear();
+    return MMA_OK;
+}
+
+// step_gcmma (mma.rs:666-769): the conservative inner loop.  The subproblem
+// is solved with rho0 (objective) and rho (constraints) raised until the
+// approximations at the trial point bound the true values from above
+// (within epsimin), or max_conservative inner iterations have run.
+mma_status mma_step_gcmma(mma_handle* h, const double* x_k, const double* x_km1, const double* x_km2, double f0,
+                          const double* df0dx, const double* fs, const double* dfsdx, mma_eval_fn eval_true,
+                          void* ctx, double* x_new, mma_info_t* info) {
+    if (!h) return fail(nullptr, MMA_E_CONTRACT, "MMA: handle is NULL");
+    const auto t0 = std::chrono::steady_clock::now();
+    try {
+        if (!h->gcmma) return mma_step(h, x_k, x_km1, x_km2, f0, df0dx, fs, dfsdx, x_new, info);
+        if (!eval_true) throw ContractError("GCMMA: eval_true must not be NULL");
+        const mma_gcmma_options_t& g = h->g;
+        const int64_t n = h->n, m = h->m;
+        const Vec xk = begin_step(h, x_k, x_km1, x_km2, f0, df0dx, fs, dfsdx, x_new);
+        // initial rho from the spans of the gradients (mma.rs:688-695)
+        double s0 = 0.0;
+        Vec sr(m, 0.0);
+        for (int64_t i = 0; i < n; ++i) {
+            const double span = h->x_max[i] - h->x_min[i];
+            s0 += std::fabs(df0dx[i]) * span;
+            for (int64_t j = 0; j < m; ++j) sr[j] += std::fabs(dfsdx[(size_t)j * n + i]) * span;
+        }
+        double rho0 = std::max(g.rho_min, g.rho_init * s0 / (double)n);
+        Vec rho(m);
+        for (int64_t j = 0; j < m; ++j) rho[j] = std::max(g.rho_min, g.rho_init * sr[j] / (double)n);
+        // psi of rows (p, q) at x (psi_rows, mma.rs:624-629)
+        auto psi = [&](const double* p, const double* q, const double* xx) {
+            double acc = 0.0;
+#pragma omp parallel for reduction(+ : acc) schedule(static)
+            for (int64_t i = 0; i < n; ++i) acc += p[i] / (h->upp[i] - xx[i]) + q[i] / (xx[i] - h->low[i]);
+            return acc;
+        };
+        int64_t inner = 0, nonfinite = 0;
+        bool conservative = false;
+        Vec fnew(m);
+        for (;;) {
+            build_sub(h, xk, df0dx, fs, dfsdx, rho0, rho);
+            h->solve_subproblem();
+            const double r0 = f0 - psi(h->p0.data(), h->q0.data(), xk.data());
+            const double f0app = r0 + psi(h->p0.data(), h->q0.data(), h->x.data());
+            Vec fapp(m);
+            for (int64_t j = 0; j < m; ++j)
+                fapp[j] = psi(&h->P[(size_t)j * n], &h->Q[(size_t)j * n], h->x.data()) - h->b[j];
+            double f0new = 0.0;
+            if (eval_true(h->x.data(), &f0new, fnew.data(), ctx) != 0)
+                throw RuntimeError("GCMMA: eval_true reported a failure");
+            bool finite = std::isfinite(f0new);
+            for (int64_t j = 0; j < m; ++j) finite = finite && std::isfinite(fnew[j]);
+            if (!finite) {
+                ++nonfinite;
+                if (inner >= g.max_conservative) break;
+                ++inner;
+                rho0 *= g.rho_growth;
+                for (double& r : rho) r *= g.rho_growth;
+                continue;
+            }
+            const bool bad0 = f0app + h->o.epsimin < f0new;
+            std::vector<char> bad(m);
+            bool any = bad0;
+            for (int64_t j = 0; j < m; ++j) {
+                bad[j] = fapp[j] + h->o.epsimin < fnew[j];
+                any = any || bad[j];
+            }
+            if (!any) {
+                conservative = true;
+                break;
+            }
+            if (inner >= g.max_conservative) break;
+            ++inner;
+            double w = 0.0;
+#pragma omp parallel for reduction(+ : w) schedule(static)
+            for (int64_t i = 0; i < n; ++i) {
+                const double xv = h->x[i], l = h->low[i], u = h->upp[i];
+                const double xxux = (xv - xk[i]) / (u - xv), xxxl = (xv - xk[i]) / (xv - l);
+                w += (xxux * xxxl) * ((u - l) / h->xmami[i]);
+            }
+            w = std::max(w, 1e-12);
+            if (bad0) rho0 = std::min(1.1 * (rho0 + (f0new - f0app) / w), g.rho_growth * rho0);
+            for (int64_t j = 0; j < m; ++j)
+                if (bad[j]) rho[j] = std::min(1.1 * (rho[j] + (fnew[j] - fapp[j]) / w), g.rho_growth * rho[j]);
+        }
+        h->nonfinite_trials += nonfinite;
+        h->rho_last.assign(1, rho0);
+        h->rho_last.insert(h->rho_last.end(), rho.begin(), rho.end());
+        finish_step(h, x_new, info, t0, inner, conservative);
+        return MMA_OK;
+    } catch (const ContractError& e) {
+        return fail(h, MMA_E_CONTRACT, e.what());
+    } catch (const std::exception& e) {
+        return fail(h, MMA_E_RUNTIME, e.what());
+    }
+}
+
+int64_t mma_gcmma_state(const mma_handle* h, double* rho, int64_t* nonfinite_trials) {
+    if (!h || !h->gcmma) return -1;
+    if (rho) std::copy(h->rho_last.begin(), h->rho_last.end(), rho);
+    if (nonfinite_trials) *nonfinite_trials = h->nonfinite_trials;
+    return (int64_t)h->rho_last.size();
 }
 
 int64_t mma_state(const mma_handle* h, double* lam, double* y, double* z, double* low, double* upp) {

@@ -48,11 +48,26 @@ class Info(C.Structure):
         ("z", C.c_double),
         ("newton_steps", C.c_int64),
         ("wallclock_s", C.c_double),
+        ("inner_iterations", C.c_int64),
+        ("conservative", C.c_int32),
     ]
 
 
+class GcmmaOptions(C.Structure):
+    _fields_ = [
+        ("rho_min", C.c_double),
+        ("rho_init", C.c_double),
+        ("rho_growth", C.c_double),
+        ("max_conservative", C.c_int64),
+    ]
+
+
+# int eval_true(const double* x, double* f0, double* fs, void* ctx)
+EVAL_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p)
+
+
 EXPORTS = ["mma_default_options", "mma_create", "mma_destroy", "mma_last_error", "mma_step", "mma_kkt_residual",
-           "mma_state"]
+           "mma_state", "mma_gcmma_default_options", "mma_enable_gcmma", "mma_step_gcmma", "mma_gcmma_state"]
 
 _lib = None
 
@@ -81,6 +96,15 @@ def load(path: Path | str | None = None) -> C.CDLL:
     lib.mma_kkt_residual.restype = C.c_double
     lib.mma_state.argtypes = [C.c_void_p, dp, dp, dp, dp, dp]
     lib.mma_state.restype = C.c_int64
+    lib.mma_gcmma_default_options.argtypes = [C.POINTER(GcmmaOptions)]
+    lib.mma_gcmma_default_options.restype = None
+    lib.mma_enable_gcmma.argtypes = [C.c_void_p, C.POINTER(GcmmaOptions)]
+    lib.mma_enable_gcmma.restype = C.c_int
+    lib.mma_step_gcmma.argtypes = [C.c_void_p, dp, dp, dp, C.c_double, dp, dp, dp, EVAL_FN, C.c_void_p, dp,
+                                   C.POINTER(Info)]
+    lib.mma_step_gcmma.restype = C.c_int
+    lib.mma_gcmma_state.argtypes = [C.c_void_p, dp, C.POINTER(C.c_int64)]
+    lib.mma_gcmma_state.restype = C.c_int64
     if path is None:
         _lib = lib
     return lib
@@ -113,12 +137,24 @@ class StepInfo:
     z: float
     newton_steps: int
     wallclock_s: float
+    inner_iterations: int = 0
+    conservative: bool = True
+
+
+def default_gcmma_options() -> dict:
+    g = GcmmaOptions()
+    load().mma_gcmma_default_options(C.byref(g))
+    return {k: getattr(g, k) for k, _ in GcmmaOptions._fields_}
 
 
 class MmaOptimizer:
-    """MMA for min f0(x) s.t. f_j(x) <= 0 (j < m), x_min <= x <= x_max."""
+    """MMA for min f0(x) s.t. f_j(x) <= 0 (j < m), x_min <= x <= x_max.
 
-    def __init__(self, n: int, m: int, x_min=0.0, x_max=1.0, a=None, c=None, d=None, **options):
+    ``gcmma`` (a dict of GcmmaOptions fields, or True for the defaults) makes
+    it the reference's GCMMA optimiser (``MmaOptimizer::gcmma``): ``step``
+    then refuses and ``step_gcmma`` runs the conservative inner loop."""
+
+    def __init__(self, n: int, m: int, x_min=0.0, x_max=1.0, a=None, c=None, d=None, gcmma=None, **options):
         self.lib = load()
         self.n, self.m = int(n), int(m)
         o = Options()
@@ -140,6 +176,14 @@ class MmaOptimizer:
         self._check(st, None)
         self.h = h
         self.last: StepInfo | None = None
+        if gcmma is not None and gcmma is not False:
+            g = GcmmaOptions()
+            self.lib.mma_gcmma_default_options(C.byref(g))
+            for k, v in (gcmma.items() if isinstance(gcmma, dict) else ()):
+                if not hasattr(g, k):
+                    raise ContractError(f"GCMMA: unknown option {k}")
+                setattr(g, k, v)
+            self._check(self.lib.mma_enable_gcmma(self.h, C.byref(g)), self.h)
 
     def _check(self, st: int, h):
         if st == MMA_OK:
@@ -171,9 +215,57 @@ class MmaOptimizer:
         st = self.lib.mma_step(self.h, _p(xk), _p(x1), _p(x2), float(f0), _p(g0), _p(f), _p(df), _p(out),
                                C.byref(info))
         self._check(st, self.h)
-        self.last = StepInfo(info.iteration, info.kkt_residual, info.subproblem_kkt, bool(info.subproblem_converged),
-                             info.subproblem_ip_residual, info.z, info.newton_steps, info.wallclock_s)
+        self.last = self._info(info)
         return out
+
+    @staticmethod
+    def _info(info) -> StepInfo:
+        return StepInfo(info.iteration, info.kkt_residual, info.subproblem_kkt, bool(info.subproblem_converged),
+                        info.subproblem_ip_residual, info.z, info.newton_steps, info.wallclock_s,
+                        int(info.inner_iterations), bool(info.conservative))
+
+    def step_gcmma(self, x_k, x_km1, x_km2, f0: float, df0dx, fs, dfsdx, eval_true) -> np.ndarray:
+        """One GCMMA step; eval_true(x) -> (f0, fs) gives the true values at a
+        trial point.  An exception raised by eval_true aborts the step and is
+        re-raised here."""
+        n, m = self.n, self.m
+        xk, x1, x2, g0 = (_vec(v, n, name) for v, name in
+                          ((x_k, "x_k"), (x_km1, "x_km1"), (x_km2, "x_km2"), (df0dx, "df0dx")))
+        f = _vec(fs, m, "fs")
+        df = _vec(dfsdx, m * n, "dfsdx")
+        out = np.empty(n)
+        info = Info()
+        raised = []
+
+        def cb(xp, f0p, fsp, _ctx):
+            try:
+                x = np.ctypeslib.as_array(xp, shape=(n,)).copy()
+                v0, vs = eval_true(x)
+                f0p[0] = float(v0)
+                vs = np.asarray(vs, dtype=np.float64).ravel()
+                if vs.size != m:
+                    raise ContractError(f"GCMMA: eval_true returned {vs.size} constraint values, expected {m}")
+                for j in range(m):
+                    fsp[j] = float(vs[j])
+                return 0
+            except BaseException as e:  # noqa: BLE001  (re-raised after the C call returns)
+                raised.append(e)
+                return 1
+
+        fn = EVAL_FN(cb)
+        st = self.lib.mma_step_gcmma(self.h, _p(xk), _p(x1), _p(x2), float(f0), _p(g0), _p(f), _p(df), fn, None,
+                                     _p(out), C.byref(info))
+        if raised:
+            raise raised[0]
+        self._check(st, self.h)
+        self.last = self._info(info)
+        return out
+
+    def gcmma_state(self) -> dict:
+        rho = np.empty(self.m + 1)
+        nf = C.c_int64()
+        k = self.lib.mma_gcmma_state(self.h, _p(rho), C.byref(nf))
+        return {"rho": rho[:max(k, 0)], "nonfinite_trials": int(nf.value)}
 
     def kkt_residual(self, x, df0dx, fs=None, dfsdx=None) -> float:
         n, m = self.n, self.m

@@ -5,8 +5,10 @@ Mirrors the reference's MMA driver (crates/implexity-jobs/src/optimize/
 mma_driver.rs): the objective and constraints are scaled once, at the first
 iterate (``calibrate``, :199-251: s0 = 1/max(|f0|, 1e-8), s_j = 1/max(|f_j|,
 1), c_j = max(1000, 10 max|s0 df0| / max|s_j df_j|)), and every step hands
-the scaled values to ``MmaOptimizer::step`` (:288-345; the plain MMA path,
-without the conservative GCMMA inner loop).  The design variables are the
+the scaled values to ``MmaOptimizer::step`` (:288-345), or, with ``gcmma``,
+to ``MmaOptimizer::step_gcmma`` (mma.rs:666-769), whose conservative inner
+loop evaluates the true objective and constraint at each trial design (one
+forward solve and the responses; no adjoint).  The design variables are the
 editable cells' raw densities in [0, 1]; the constraint is the reference's
 volume-fraction residual v_mean / t - 1 <= 0 with v_mean the mean design
 density phi over the cells and t the target fraction (spec.rs:782-790,
@@ -32,7 +34,8 @@ from .solver import LbmSolver
 
 
 class DesignLoop:
-    def __init__(self, problem: dict, weights, volume_fraction: float = 0.4, mma_options: dict | None = None):
+    def __init__(self, problem: dict, weights, volume_fraction: float = 0.4, mma_options: dict | None = None,
+                 gcmma: bool | dict = False):
         self.norm = normalize(problem)
         self.shape = tuple(self.norm.shape)
         self.w = np.asarray(weights, float)
@@ -48,6 +51,8 @@ class DesignLoop:
         self.s = None
         self.c = None
         self.mma_options = dict(mma_options or {})
+        self.gcmma = gcmma
+        self.trial_evaluations = 0
 
     def close(self):
         self.solver.close()
@@ -83,7 +88,24 @@ class DesignLoop:
             gj = float(np.max(np.abs(self.s[j] * dfs[j]))) if dfs[j].size else 0.0
             c.append(max(1000.0, 10.0 * g0 / gj) if gj > 0.0 else 1000.0)
         self.c = np.array(c)
-        self.opt = MmaOptimizer(self.n, len(fs), x_min=0.0, x_max=1.0, c=self.c, **self.mma_options)
+        self.opt = MmaOptimizer(self.n, len(fs), x_min=0.0, x_max=1.0, c=self.c,
+                                gcmma=self.gcmma if self.gcmma else None, **self.mma_options)
+
+    def true_values(self, raw: np.ndarray):
+        """The objective and the volume constraint of a trial design (the
+        GCMMA inner loop's eval_true): forward solve and responses only.  A
+        design whose evaluation is refused (admission) reads as non-finite,
+        which makes GCMMA raise rho and retry."""
+        s = self.solver
+        self.trial_evaluations += 1
+        s.set_design(raw)
+        try:
+            s.forward()
+        except ContractError:
+            return float("nan"), np.array([float("nan")])
+        r = s.responses()
+        con = r[5] / (self.cells * self.dv) / self.vf - 1.0
+        return float(np.dot(self.w, r)), np.array([con])
 
     def run(self, raw0: np.ndarray, iterations: int, log=None) -> dict:
         raw = np.array(raw0, dtype=float).reshape(self.shape)
@@ -108,12 +130,24 @@ class DesignLoop:
             if self.s0 is None:
                 self.calibrate(f0, df0, fs, dfs)
             t1 = time.perf_counter()
-            xn = self.opt.step(x, xm1, xm2, self.s0 * f0, self.s0 * df0, self.s * fs, (self.s[:, None] * dfs).ravel())
+            if self.gcmma:
+                def eval_true(xt):
+                    trial = raw.copy()
+                    trial[self.free] = xt
+                    tf0, tfs = self.true_values(trial)
+                    return self.s0 * tf0, self.s * tfs
+
+                xn = self.opt.step_gcmma(x, xm1, xm2, self.s0 * f0, self.s0 * df0, self.s * fs,
+                                         (self.s[:, None] * dfs).ravel(), eval_true)
+            else:
+                xn = self.opt.step(x, xm1, xm2, self.s0 * f0, self.s0 * df0, self.s * fs,
+                                   (self.s[:, None] * dfs).ravel())
             t2 = time.perf_counter()
             info = self.opt.last
             rec = {"iteration": it, "objective": f0, "volume_fraction": (con + 1.0) * self.vf,
                    "kkt_residual": info.kkt_residual, "max_move": float(np.max(np.abs(xn - x))),
-                   "mma_s": t2 - t1, "mma_newton_steps": info.newton_steps, "wall_s": t2 - t0, **timing}
+                   "mma_s": t2 - t1, "mma_newton_steps": info.newton_steps, "wall_s": t2 - t0,
+                   "gcmma_inner": info.inner_iterations, "conservative": info.conservative, **timing}
             history.append(rec)
             if log:
                 log(rec)
@@ -141,9 +175,11 @@ def main():
     ap.add_argument("--storage", choices=["float32", "float16"], default="float32")
     ap.add_argument("--volume-fraction", type=float, default=0.4)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--gcmma", action="store_true", help="conservative GCMMA steps (MmaOptimizer::step_gcmma)")
     a = ap.parse_args()
     shape = tuple(a.shape)
-    loop = DesignLoop(c5_problem(shape, a.forward_steps, a.storage), workloads.objective_weights(), a.volume_fraction)
+    loop = DesignLoop(c5_problem(shape, a.forward_steps, a.storage), workloads.objective_weights(), a.volume_fraction,
+                      gcmma=a.gcmma)
     try:
         out = loop.run(c5_initial_design(shape, a.seed), a.iterations,
                        log=lambda r: print(json.dumps(r), flush=True))

@@ -11,6 +11,9 @@
  *                      sub_kkt :1133-1148)
  *   mma_kkt_residual  MmaOptimizer::kkt_residual   mma.rs:420-476
  *   mma_state         MmaOptimizer::state_dict     mma.rs:377-387
+ *   mma_enable_gcmma  MmaOptimizer::gcmma          mma.rs:339-355
+ *   mma_step_gcmma    MmaOptimizer::step_gcmma     mma.rs:666-769
+ *   mma_gcmma_state   GcmmaState (rho, nonfinite_trials)  mma.rs:242-248, 360-364
  * The calibration of the objective/constraint scaling and of c lives in the
  * Python driver (implexity_b200/optimize.py; mma_driver.rs:199-251).
  *
@@ -64,7 +67,23 @@ typedef struct {
     double z;
     int64_t newton_steps;         /* interior-point Newton steps of the subproblem */
     double wallclock_s;
+    int64_t inner_iterations;     /* GCMMA: conservative inner iterations (0 for a plain step) */
+    int32_t conservative;         /* GCMMA: the accepted approximation bounds the true values */
 } mma_info_t;
+
+/* GcmmaOptions (mma.rs:131-145); the defaults are those of the reference. */
+typedef struct {
+    double rho_min;           /* 1e-6 */
+    double rho_init;          /* 0.1 */
+    double rho_growth;        /* 10 */
+    int64_t max_conservative; /* 15 */
+} mma_gcmma_options_t;
+
+/* The true objective and constraint values at a trial point (the
+ * reference's EvalTrue closure): writes *f0 and fs[0..m); returns 0, or
+ * nonzero to abort the step with MMA_E_RUNTIME.  Non-finite values are not
+ * an error: the step raises rho and retries, as the reference does. */
+typedef int (*mma_eval_fn)(const double* x, double* f0, double* fs, void* ctx);
 
 typedef struct mma_handle mma_handle;
 
@@ -86,6 +105,21 @@ MMA_API double mma_kkt_residual(const mma_handle* h, const double* x, const doub
 /* Multipliers and asymptotes of the last step: lam, y (m each), z, L, U (n
  * each); any pointer may be NULL.  Returns the iteration count. */
 MMA_API int64_t mma_state(const mma_handle* h, double* lam, double* y, double* z, double* low, double* upp);
+
+/* GCMMA.  mma_enable_gcmma turns a handle into a GCMMA optimiser (options
+ * NULL: the defaults); mma_step then refuses, as MmaOptimizer::step does for
+ * a GCMMA optimiser, and mma_step_gcmma runs the conservative inner loop,
+ * calling eval_true once per inner iteration.  mma_step_gcmma on a plain
+ * handle is mma_step. */
+MMA_API void mma_gcmma_default_options(mma_gcmma_options_t* g);
+MMA_API mma_status mma_enable_gcmma(mma_handle* h, const mma_gcmma_options_t* g);
+MMA_API mma_status mma_step_gcmma(mma_handle* h, const double* x_k, const double* x_km1, const double* x_km2,
+                                  double f0, const double* df0dx, const double* fs, const double* dfsdx,
+                                  mma_eval_fn eval_true, void* ctx, double* x_new, mma_info_t* info);
+/* rho0 then rho[0..m) of the last GCMMA step (m + 1 values) and the count of
+ * trial points with non-finite true values so far.  Returns m + 1, 0 before
+ * the first step, -1 for a plain handle. */
+MMA_API int64_t mma_gcmma_state(const mma_handle* h, double* rho, int64_t* nonfinite_trials);
 
 #ifdef __cplusplus
 }

@@ -181,7 +181,7 @@ def test_ctypes_layouts_match_the_header(tmp_path):
     structs = {"lbm_port_t": _abi.Port, "lbm_problem_t": _abi.Problem, "lbm_diag_t": _abi.Diag,
                "lbm_adjoint_opts_t": _abi.AdjointOpts, "lbm_adjoint_report_t": _abi.AdjointReport,
                "lbm_info_t": _abi.Info, "lbm_slab_diag_t": _abi.SlabDiag, "mma_options_t": mma.Options,
-               "mma_info_t": mma.Info}
+               "mma_info_t": mma.Info, "mma_gcmma_options_t": mma.GcmmaOptions}
     lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "lbm_b200.h"', '#include "mma_cpu.h"',
              "int main(void) {"]
     for cname, py in structs.items():

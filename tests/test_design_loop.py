@@ -25,3 +25,22 @@ def test_design_loop_small_channel(gpu_lib):
     # the initial design (~0.52) violates the 0.4 volume bound; MMA moves toward it
     assert h[-1]["volume_fraction"] < h[0]["volume_fraction"]
     assert all(r["adjoint_iterations"] > 0 for r in h)
+
+
+def test_design_loop_gcmma_small_channel(gpu_lib):
+    """The GCMMA path of the loop: every trial design is evaluated by a forward
+    solve, the accepted approximations are conservative (or the inner loop
+    ran out), and the volume moves toward its bound."""
+    shape = (24, 12, 12)
+    loop = DesignLoop(c5_problem(shape, forward_steps=400), workloads.objective_weights(), volume_fraction=0.4,
+                      gcmma=True)
+    try:
+        out = loop.run(c5_initial_design(shape, 0), iterations=3)
+    finally:
+        loop.close()
+    h = out["history"]
+    assert len(h) == 3
+    assert np.all(np.isfinite([r["objective"] for r in h]))
+    assert loop.trial_evaluations == sum(r["gcmma_inner"] + 1 for r in h)
+    assert all(r["conservative"] or r["gcmma_inner"] == 15 for r in h)
+    assert h[-1]["volume_fraction"] < h[0]["volume_fraction"]
