@@ -35,7 +35,7 @@ from .solver import LbmSolver
 
 class DesignLoop:
     def __init__(self, problem: dict, weights, volume_fraction: float = 0.4, mma_options: dict | None = None,
-                 gcmma: bool | dict = False):
+                 gcmma: bool | dict = False, adjoint_max_iterations: int = 1_000_000):
         self.norm = normalize(problem)
         self.shape = tuple(self.norm.shape)
         self.w = np.asarray(weights, float)
@@ -52,6 +52,9 @@ class DesignLoop:
         self.c = None
         self.mma_options = dict(mma_options or {})
         self.gcmma = gcmma
+        # the Neumann count of the long C5 channel grows as the design opens
+        # (89 000 at the first iterate, ~98 000 by the eighth at 512x256x256)
+        self.adjoint_max_iterations = int(adjoint_max_iterations)
         self.trial_evaluations = 0
 
     def close(self):
@@ -68,7 +71,7 @@ class DesignLoop:
         r = s.responses()
         t1 = time.perf_counter()
         g, rep = s.gradient(self.w, mode="steady", tolerance=1e-8, lambda_storage=self.norm.options.storage,
-                            check_every=100)
+                            check_every=100, max_iterations=self.adjoint_max_iterations)
         t2 = time.perf_counter()
         v_mean = r[5] / (self.cells * self.dv)
         dres = s.design_vjp(np.full(self.shape, 1.0 / (self.cells * self.vf)))
