@@ -25,8 +25,12 @@ struct AdjStage {
 
 // STG = 1: the stage-objective variant, which reads the second moments of
 // the recorded state as well and adds the state's response VJP.
+// Residency: D3Q19 with 16-bit storage runs three blocks per SM (72
+// registers, a few spilled): its step is bound by latency and instruction
+// issue, not bytes, and a third block's warps hide more of it; the others
+// keep two blocks and their registers.
 template <int Q, int COLL, typename T, int AL, int STG>
-__global__ void __launch_bounds__(TPB, 2) k_adjoint(AdjArgs a) {
+__global__ void __launch_bounds__(TPB, (sizeof(T) == 2 && Q == 19 ? 3 : 2)) k_adjoint(AdjArgs a) {
     constexpr int NREC = STG ? 10 : 4;
     using S = AdjStage<Q, T, NREC>;
     constexpr int NCOPY = Q + NREC + 2;  // runs of lambda, the record, mask and alpha
