@@ -881,16 +881,19 @@ __device__ __forceinline__ float collide_vjp(float (&gb)[Q], float rp, const flo
     float F[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) F[d] = rho * (P.a[d] - alpha * u[d]);
-    // weighted moments of gb and z = R^T gb (TRT part), pair by pair
+    // weighted moments of gb, pair by pair; the pair sums and differences are
+    // kept for the output pass, which applies the TRT part of the transpose
+    // (gb - R^T gb per pair: (1 - om)/2 sm +- (1 - omm)/2 df)
     float M0 = L::w(0) * gb[0];
     float M1[3] = {0.f, 0.f, 0.f}, M2[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    float z[Q];
-    z[0] = om * gb[0];
+    float SM[NP], DF[NP];
+    float g0 = (1.f - om) * gb[0];  // the rest population's output, less rho_bar
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
         const int i = k + 1, o = opp<Q>(i);
         const float sm = gb[i] + gb[o], df = gb[i] - gb[o];
-        constexpr float half = 0.5f;
+        SM[k] = sm;
+        DF[k] = df;
         const float w = L::w(i);
         const int c0 = L::cx(i), c1 = L::cy(i), c2 = L::cz(i);
         M0 = fmaf(w, sm, M0);
@@ -909,9 +912,6 @@ __device__ __forceinline__ float collide_vjp(float (&gb)[Q], float rp, const flo
         if (c0 && c1) M2[3] = fmaf(w * c0 * c1, sm, M2[3]);
         if (c0 && c2) M2[4] = fmaf(w * c0 * c2, sm, M2[4]);
         if (c1 && c2) M2[5] = fmaf(w * c1 * c2, sm, M2[5]);
-        const float a = half * om * sm, b = half * omm * df;
-        z[i] = a + b;
-        z[o] = a - b;
     }
     float Z0 = om * M0, H0 = (1.f - 0.5f * om) * M0;
     float Z1[3], H1[3], Z2[6], H2[6];
@@ -925,43 +925,38 @@ __device__ __forceinline__ float collide_vjp(float (&gb)[Q], float rp, const flo
         Z2[e] = om * M2[e];
         H2[e] = (1.f - 0.5f * om) * M2[e];
     }
+    float bulk_c = 0.f;  // MRT_BULK: the bulk correction's coefficient
     if constexpr (COLL == CK_MRT_BULK) {
         // the bulk correction folded: b_i = |c_i|^2 - 1, |b|^2_W = 2/3,
         // sum_i w_i b_i = 0 and sum_i w_i b_i c_ia c_ib = 2/9 delta_ab on both lattices
         float e = -L::w(0) * gb[0];
 #pragma unroll
         for (int k = 0; k < NP; ++k) {
-            const int i = k + 1, o = opp<Q>(i);
+            const int i = k + 1;
             const int c2 = L::cx(i) * L::cx(i) + L::cy(i) * L::cy(i) + L::cz(i) * L::cz(i);
-            if (c2 != 1) e = fmaf(L::w(i) * (float)(c2 - 1), gb[i] + gb[o], e);  // folded after unrolling
+            if (c2 != 1) e = fmaf(L::w(i) * (float)(c2 - 1), SM[k], e);  // folded after unrolling
         }
-        const float c = P.proj_rate[0] * e * 1.5f;
-        z[0] -= c;
-#pragma unroll
-        for (int k = 0; k < NP; ++k) {
-            const int i = k + 1, o = opp<Q>(i);
-            const int c2 = L::cx(i) * L::cx(i) + L::cy(i) * L::cy(i) + L::cz(i) * L::cz(i);
-            if (c2 != 1) {
-                z[i] = fmaf(c, (float)(c2 - 1), z[i]);
-                z[o] = fmaf(c, (float)(c2 - 1), z[o]);
-            }
-        }
+        bulk_c = P.proj_rate[0] * e * 1.5f;
+        const float c = bulk_c;
+        g0 += c;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             Z2[d] = fmaf(c, 2.f / 9.f, Z2[d]);
             H2[d] = fmaf(-0.5f * c, 2.f / 9.f, H2[d]);
         }
     }
+    float cproj[MAX_PROJ];  // MRT: the rank-one corrections' coefficients
     if constexpr (COLL == CK_MRT) {
 #pragma unroll
         for (int p = 0; p < MAX_PROJ; ++p) {
+            cproj[p] = 0.f;
             if (p < P.n_proj) {
                 float e = 0.f;
 #pragma unroll
                 for (int i = 0; i < Q; ++i) e = fmaf(P.proj_left[p][i], gb[i], e);
                 const float c = P.proj_rate[p] * e;
-#pragma unroll
-                for (int i = 0; i < Q; ++i) z[i] = fmaf(c, P.proj_right[p][i], z[i]);
+                cproj[p] = c;
+                g0 = fmaf(-c, P.proj_right[p][0], g0);
                 Z0 = fmaf(c, P.proj_m0[p], Z0);
                 H0 = fmaf(-0.5f * c, P.proj_m0[p], H0);
 #pragma unroll
@@ -1009,13 +1004,34 @@ __device__ __forceinline__ float collide_vjp(float (&gb)[Q], float rp, const flo
         sbar -= ub[d] * u[d] * inv_s;
     }
     abar += 0.5f * sbar;
+    // output: gb - R^T gb + rho_bar + c . mb, pair by pair (with the MRT
+    // corrections, which are even: the same for i and opp(i))
+    const float hp = 0.5f * (1.f - om), hm = 0.5f * (1.f - omm);
+    gb[0] = g0 + rho_bar;
 #pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        float v = gb[i] - z[i] + rho_bar;
-        if (L::cx(i)) v += L::cx(i) * mb[0];
-        if (L::cy(i)) v += L::cy(i) * mb[1];
-        if (L::cz(i)) v += L::cz(i) * mb[2];
-        gb[i] = v;
+    for (int k = 0; k < NP; ++k) {
+        const int i = k + 1, o = opp<Q>(i);
+        float base = rho_bar;
+        if constexpr (COLL == CK_MRT_BULK) {
+            const int c2 = L::cx(i) * L::cx(i) + L::cy(i) * L::cy(i) + L::cz(i) * L::cz(i);
+            if (c2 != 1) base = fmaf(-bulk_c, (float)(c2 - 1), base);  // folded after unrolling
+        }
+        float pi = fmaf(hp, SM[k], base), po = pi;
+        if constexpr (COLL == CK_MRT) {
+#pragma unroll
+            for (int p = 0; p < MAX_PROJ; ++p)
+                if (p < P.n_proj) {
+                    pi = fmaf(-cproj[p], P.proj_right[p][i], pi);
+                    po = fmaf(-cproj[p], P.proj_right[p][o], po);
+                }
+        }
+        float cm = 0.f;
+        if (L::cx(i)) cm = fmaf((float)L::cx(i), mb[0], cm);
+        if (L::cy(i)) cm = fmaf((float)L::cy(i), mb[1], cm);
+        if (L::cz(i)) cm = fmaf((float)L::cz(i), mb[2], cm);
+        const float d = fmaf(hm, DF[k], cm);
+        gb[i] = pi + d;
+        gb[o] = po - d;
     }
     return abar;
 }
