@@ -11,6 +11,7 @@
 // the cell's own slots of the other array.  Loads are staged like the
 // forward step (lbm_device.cuh).
 #include "lbm_device.cuh"
+#include "lbm_vec2.cuh"
 
 namespace lbm {
 namespace {
@@ -25,12 +26,19 @@ struct AdjStage {
 
 // STG = 1: the stage-objective variant, which reads the second moments of
 // the recorded state as well and adds the state's response VJP.
-// Residency: D3Q19 with 16-bit storage runs three blocks per SM (72
-// registers, a few spilled): its step is bound by latency and instruction
-// issue, not bytes, and a third block's warps hide more of it; the others
-// keep two blocks and their registers.
-template <int Q, int COLL, typename T, int AL, int STG>
-__global__ void __launch_bounds__(TPB, (sizeof(T) == 2 && Q == 19 ? 3 : 2)) k_adjoint(AdjArgs a) {
+// LN = 2 (D3Q19, 16-bit storage, TRT/BGK or the folded bulk MRT, no stage
+// seeds): four consumer warps whose threads take two cells each, c and
+// c + 128 of the tile, and run the collision transpose for both at once in
+// packed FP32 pairs (collide_vjp_lanes, lbm_vec2.cuh); cells that need the
+// general path (solid, periodic face, port, per-cell tau) take the one-lane
+// body one after the other.  The 16-bit step is bound by instruction issue,
+// and the packed pairs halve its arithmetic.
+// Residency: three blocks per SM for 16-bit D3Q19 (LN = 1: 72 registers;
+// LN = 2: 160 threads with up to 136 registers); the others keep two blocks.
+template <int Q, int COLL, typename T, int AL, int STG, int LN>
+__global__ void __launch_bounds__(32 + 32 * (CONSUMER_WARPS / LN), (sizeof(T) == 2 && Q == 19 ? 3 : 2))
+    k_adjoint(AdjArgs a) {
+    constexpr int CW = CONSUMER_WARPS / LN;  // consumer warps
     constexpr int NREC = STG ? 10 : 4;
     using S = AdjStage<Q, T, NREC>;
     constexpr int NCOPY = Q + NREC + 2;  // runs of lambda, the record, mask and alpha
@@ -48,7 +56,7 @@ __global__ void __launch_bounds__(TPB, (sizeof(T) == 2 && Q == 19 ? 3 : 2)) k_ad
 #pragma unroll
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], CONSUMER_WARPS);
+            mbar_init(&empty[s], CW);
         }
         mbar_fence_init();
     }
@@ -83,83 +91,136 @@ __global__ void __launch_bounds__(TPB, (sizeof(T) == 2 && Q == 19 ? 3 : 2)) k_ad
             }
         }
     } else {
-        const int c = threadIdx.x - 32;
+        const int c0 = threadIdx.x - 32;
         int s = 0;
         uint32_t round = 0;
         const float s_in = 1.f / a.in_scale_inv;        // stored scale of the input
         const float k_out = a.out_scale * a.in_scale_inv;  // stored input -> stored output
-        for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-            const uint32_t x = tile * TILE + c;
-            // the running alpha cotangent, read before the wait so that its
-            // latency hides behind the staged copies and the collision
-            const float ab_prev = (!a.overwrite_abar && x < n) ? a.abar[x] : 0.f;
-            const bool ok = mbar_wait(&full[s], round & 1u, a.err);
-            const S* st = stage_at<S>(smem, s);
-            const uint32_t m = ok && x < n ? st->mask[c] : MASK_SOLID;
+        // one cell c of the staged tile (mask m, the running alpha cotangent ab_prev)
+        auto one_cell = [&](const S* st, int c, uint32_t x, uint32_t m, float ab_prev) {
             const bool fluid = !(m & MASK_SOLID);
+            if (!fluid) return;
             float v[Q];
-            if (fluid) {
-                if (!(m & MASK_WRAP)) {
+            if (!(m & MASK_WRAP)) {
 #pragma unroll
-                    for (int q = 0; q < Q; ++q)
-                        v[q] = Cvt<T>::to(st->run[q][(AL ? rund_aligned<Q, T, 1>(q) : a.rund[q]) + c]);
-                    if (m & LINK_BITS) {
-                        // transposed bounce-back: the cell's own opposite slot
+                for (int q = 0; q < Q; ++q)
+                    v[q] = Cvt<T>::to(st->run[q][(AL ? rund_aligned<Q, T, 1>(q) : a.rund[q]) + c]);
+                if (m & LINK_BITS) {
+                    // transposed bounce-back: the cell's own opposite slot
 #pragma unroll
-                        for (int q = 1; q < Q; ++q)
-                            if ((m >> opp<Q>(q)) & 1u) v[q] = Cvt<T>::to(B[opp<Q>(q) * n + x]);
-                    }
-                } else {
+                    for (int q = 1; q < Q; ++q)
+                        if ((m >> opp<Q>(q)) & 1u) v[q] = Cvt<T>::to(B[opp<Q>(q) * n + x]);
+                }
+            } else {
 #pragma unroll
-                    for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(B[pull_adj_index<Q>(a.G, x, m, q)]);
+                for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(B[pull_adj_index<Q>(a.G, x, m, q)]);
+            }
+            const float u[3] = {st->rec[1][a.recd[1] + c], st->rec[2][a.recd[2] + c], st->rec[3][a.recd[3] + c]};
+            const float rp = st->rec[0][a.recd[0] + c];
+            // v stays in the stored scale (the transposed step is linear): the
+            // alpha cotangent is rescaled once, the output by out_scale / in_scale
+            float om = a.P.omega, omm = a.P.om;
+            if (a.omega_cell) om = omm = a.omega_cell[x];  // Tau::PerCell (BGK only)
+            float ab = collide_vjp<Q, COLL>(v, rp, u, st->alpha[c], a.P, om, omm) * a.in_scale_inv;
+            if constexpr (STG) {
+                if (a.stage) {
+                    // the stage seed of this state: d(w . responses)/dg from its record
+                    float Sm[6], fb[Q];
+#pragma unroll
+                    for (int e = 0; e < 6; ++e) Sm[e] = st->rec[4 + e][a.recd[4 + e] + c];
+                    const PortMap* pm = (m & MASK_PORT) ? &a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1] : nullptr;
+                    ab += response_vjp<Q>(rp, u, Sm, st->alpha[c], pm ? pm->dp_weight : 0.f, pm != nullptr, a.seed,
+                                          a.P, fb);
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) v[q] = fmaf(fb[q], s_in, v[q]);
                 }
             }
-            if (fluid) {
-                const float u[3] = {st->rec[1][a.recd[1] + c], st->rec[2][a.recd[2] + c], st->rec[3][a.recd[3] + c]};
-                const float rp = st->rec[0][a.recd[0] + c];
-                // v stays in the stored scale (the transposed step is linear): the
-                // alpha cotangent is rescaled once, the output by out_scale / in_scale
-                float om = a.P.omega, omm = a.P.om;
-                if (a.omega_cell) om = omm = a.omega_cell[x];  // Tau::PerCell (BGK only)
-                float ab = collide_vjp<Q, COLL>(v, rp, u, st->alpha[c], a.P, om, omm) * a.in_scale_inv;
-                if constexpr (STG) {
-                    if (a.stage) {
-                        // the stage seed of this state: d(w . responses)/dg from its record
-                        float Sm[6], fb[Q];
-#pragma unroll
-                        for (int e = 0; e < 6; ++e) Sm[e] = st->rec[4 + e][a.recd[4 + e] + c];
-                        const PortMap* pm = (m & MASK_PORT) ? &a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1] : nullptr;
-                        ab += response_vjp<Q>(rp, u, Sm, st->alpha[c], pm ? pm->dp_weight : 0.f, pm != nullptr, a.seed,
-                                              a.P, fb);
-#pragma unroll
-                        for (int q = 0; q < Q; ++q) v[q] = fmaf(fb[q], s_in, v[q]);
-                    }
+            a.abar[x] = fmaf(ab, a.abar_factor, ab_prev);
+            if (a.port_transpose && (m & MASK_PORT)) {
+                const PortMap& pm = a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1];
+                if (!pm.recon) {
+                    port_transpose<Q>(pm, v);
+                } else {
+                    // nonlinear ports, linearised at the recorded (rho, j / rho)
+                    // of port_lin_cell (zero acceleration: u = j / (rho (1 +
+                    // alpha / 2))); an extrapolating port's share for its
+                    // neighbour stays in this cell's slots until the move that
+                    // follows the step (launch_nee_move)
+                    const size_t xm = (size_t)port_lin_cell(pm, x);
+                    const float sc = 1.f + 0.5f * a.alpha[xm];
+                    const float um[3] = {a.record[(size_t)n + xm] * sc, a.record[2 * (size_t)n + xm] * sc,
+                                         a.record[3 * (size_t)n + xm] * sc};
+                    port_vjp<Q>(pm, a.record[xm], um, v);
                 }
-                a.abar[x] = fmaf(ab, a.abar_factor, ab_prev);
-                if (a.port_transpose && (m & MASK_PORT)) {
-                    const PortMap& pm = a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1];
-                    if (!pm.recon) {
-                        port_transpose<Q>(pm, v);
+            }
+            store_own_lam<Q, T>(D, n, x, v, k_out);
+            if (a.norm2) {
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    const float sv = v[q] * k_out;
+                    nsum += (double)sv * (double)sv;
+                }
+            }
+        };
+        for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            if constexpr (LN == 1) {
+                const uint32_t x = tile * TILE + c0;
+                // the running alpha cotangent, read before the wait so that its
+                // latency hides behind the staged copies and the collision
+                const float ab_prev = (!a.overwrite_abar && x < n) ? a.abar[x] : 0.f;
+                const bool ok = mbar_wait(&full[s], round & 1u, a.err);
+                const S* st = stage_at<S>(smem, s);
+                one_cell(st, c0, x, ok && x < n ? st->mask[c0] : MASK_SOLID, ab_prev);
+            } else {
+                const int cA = c0, cB = c0 + 32 * CW;
+                const uint32_t xA = tile * TILE + cA, xB = tile * TILE + cB;
+                const float pA = (!a.overwrite_abar && xA < n) ? a.abar[xA] : 0.f;
+                const float pB = (!a.overwrite_abar && xB < n) ? a.abar[xB] : 0.f;
+                const bool ok = mbar_wait(&full[s], round & 1u, a.err);
+                const S* st = stage_at<S>(smem, s);
+                const uint32_t mA = ok && xA < n ? st->mask[cA] : MASK_SOLID;
+                const uint32_t mB = ok && xB < n ? st->mask[cB] : MASK_SOLID;
+                if constexpr (COLL != CK_MRT && !STG) {
+                    if (!((mA | mB) & (MASK_SOLID | MASK_WRAP | MASK_PORT)) && !a.omega_cell) {
+                        F2 v[Q];
+#pragma unroll
+                        for (int q = 0; q < Q; ++q) {
+                            const int off = AL ? rund_aligned<Q, T, 1>(q) : a.rund[q];
+                            v[q] = {make_float2(Cvt<T>::to(st->run[q][off + cA]), Cvt<T>::to(st->run[q][off + cB]))};
+                        }
+                        if ((mA | mB) & LINK_BITS) {
+#pragma unroll
+                            for (int q = 1; q < Q; ++q) {
+                                if ((mA >> opp<Q>(q)) & 1u) v[q].v.x = Cvt<T>::to(B[opp<Q>(q) * n + xA]);
+                                if ((mB >> opp<Q>(q)) & 1u) v[q].v.y = Cvt<T>::to(B[opp<Q>(q) * n + xB]);
+                            }
+                        }
+                        F2 u[3];
+#pragma unroll
+                        for (int d = 0; d < 3; ++d)
+                            u[d] = {make_float2(st->rec[1 + d][a.recd[1 + d] + cA], st->rec[1 + d][a.recd[1 + d] + cB])};
+                        const F2 rp = {make_float2(st->rec[0][a.recd[0] + cA], st->rec[0][a.recd[0] + cB])};
+                        const F2 al = {make_float2(st->alpha[cA], st->alpha[cB])};
+                        const F2 ab = collide_vjp_lanes<Q, COLL, F2>(v, rp, u, al, a.P, a.P.omega, a.P.om, k_out);
+                        a.abar[xA] = fmaf(ab.v.x * a.in_scale_inv, a.abar_factor, pA);
+                        a.abar[xB] = fmaf(ab.v.y * a.in_scale_inv, a.abar_factor, pB);
+#pragma unroll
+                        for (int q = 0; q < Q; ++q) {
+                            D[q * n + xA] = Cvt<T>::from(v[q].v.x);
+                            D[q * n + xB] = Cvt<T>::from(v[q].v.y);
+                        }
+                        if (a.norm2) {
+#pragma unroll
+                            for (int q = 0; q < Q; ++q)
+                                nsum += (double)v[q].v.x * (double)v[q].v.x + (double)v[q].v.y * (double)v[q].v.y;
+                        }
                     } else {
-                        // nonlinear ports, linearised at the recorded (rho, j / rho)
-                        // of port_lin_cell (zero acceleration: u = j / (rho (1 +
-                        // alpha / 2))); an extrapolating port's share for its
-                        // neighbour stays in this cell's slots until the move that
-                        // follows the step (launch_nee_move)
-                        const size_t xm = (size_t)port_lin_cell(pm, x);
-                        const float sc = 1.f + 0.5f * a.alpha[xm];
-                        const float um[3] = {a.record[(size_t)n + xm] * sc, a.record[2 * (size_t)n + xm] * sc,
-                                             a.record[3 * (size_t)n + xm] * sc};
-                        port_vjp<Q>(pm, a.record[xm], um, v);
+                        one_cell(st, cA, xA, mA, pA);
+                        one_cell(st, cB, xB, mB, pB);
                     }
-                }
-                store_own_lam<Q, T>(D, n, x, v, k_out);
-                if (a.norm2) {
-#pragma unroll
-                    for (int q = 0; q < Q; ++q) {
-                        const float sv = v[q] * k_out;
-                        nsum += (double)sv * (double)sv;
-                    }
+                } else {
+                    one_cell(st, cA, xA, mA, pA);
+                    one_cell(st, cB, xB, mB, pB);
                 }
             }
             __syncwarp();
@@ -178,18 +239,27 @@ __global__ void __launch_bounds__(TPB, (sizeof(T) == 2 && Q == 19 ? 3 : 2)) k_ad
     }
 }
 
-template <int Q, int COLL, typename T, int AL, int STG>
+template <int Q, int COLL, typename T, int AL, int STG, int LN>
 cudaError_t run_adjoint_al(const AdjArgs& a, cudaStream_t s) {
     constexpr size_t smem = pipe_bytes<AdjStage<Q, T, STG ? 10 : 4>, ring_depth<AdjStage<Q, T, STG ? 10 : 4>, T>()>();
+    constexpr int threads = 32 + 32 * (CONSUMER_WARPS / LN);
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = set_smem(k_adjoint<Q, COLL, T, AL, STG>, smem);
+        cudaError_t e = set_smem(k_adjoint<Q, COLL, T, AL, STG, LN>, smem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    const int grid = persistent_grid((const void*)k_adjoint<Q, COLL, T, AL, STG>, a.G.n, smem, TPB, TILE);
-    k_adjoint<Q, COLL, T, AL, STG><<<grid, TPB, smem, s>>>(a);
+    const int grid = persistent_grid((const void*)k_adjoint<Q, COLL, T, AL, STG, LN>, a.G.n, smem, threads, TILE);
+    k_adjoint<Q, COLL, T, AL, STG, LN><<<grid, threads, smem, s>>>(a);
     return cudaGetLastError();
+}
+
+// The two-lane consumers (LN = 2) serve D3Q19 with 16-bit storage, no stage
+// seeds and a collision other than the general MRT.
+template <int Q, int COLL, typename T, int AL, int STG>
+cudaError_t run_adjoint_ln(const AdjArgs& a, cudaStream_t s) {
+    if constexpr (Q == 19 && sizeof(T) == 2 && COLL != CK_MRT && !STG) return run_adjoint_al<Q, COLL, T, AL, STG, 2>(a, s);
+    else return run_adjoint_al<Q, COLL, T, AL, STG, 1>(a, s);
 }
 
 template <int Q, typename T>
@@ -205,8 +275,8 @@ template <int Q, int COLL, typename T>
 cudaError_t run_adjoint(const AdjArgs& a, cudaStream_t s) {
     const bool al = adj_table_is_aligned<Q, T>(a.rund);
     if (a.rec_planes == 10)
-        return al ? run_adjoint_al<Q, COLL, T, 1, 1>(a, s) : run_adjoint_al<Q, COLL, T, 0, 1>(a, s);
-    return al ? run_adjoint_al<Q, COLL, T, 1, 0>(a, s) : run_adjoint_al<Q, COLL, T, 0, 0>(a, s);
+        return al ? run_adjoint_ln<Q, COLL, T, 1, 1>(a, s) : run_adjoint_ln<Q, COLL, T, 0, 1>(a, s);
+    return al ? run_adjoint_ln<Q, COLL, T, 1, 0>(a, s) : run_adjoint_ln<Q, COLL, T, 0, 0>(a, s);
 }
 
 }  // namespace
