@@ -24,6 +24,76 @@ struct AdjStage {
     float alpha[FRUN];
 };
 
+// One cell c of a staged tile of the transposed step (mask m, the running
+// alpha cotangent ab_prev): the general path.
+template <int Q, int COLL, typename T, int AL, int STG, typename S>
+__device__ __forceinline__ void adj_one_cell(const AdjArgs& a, const S* st, int c, uint32_t x, uint32_t m, float ab_prev,
+                                             const T* B, T* D, uint32_t n, float s_in, float k_out, double& nsum) {
+    const bool fluid = !(m & MASK_SOLID);
+    if (!fluid) return;
+    float v[Q];
+    if (!(m & MASK_WRAP)) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            v[q] = Cvt<T>::to(st->run[q][(AL ? rund_aligned<Q, T, 1>(q) : a.rund[q]) + c]);
+        if (m & LINK_BITS) {
+            // transposed bounce-back: the cell's own opposite slot
+#pragma unroll
+            for (int q = 1; q < Q; ++q)
+                if ((m >> opp<Q>(q)) & 1u) v[q] = Cvt<T>::to(B[opp<Q>(q) * n + x]);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(B[pull_adj_index<Q>(a.G, x, m, q)]);
+    }
+    const float u[3] = {st->rec[1][a.recd[1] + c], st->rec[2][a.recd[2] + c], st->rec[3][a.recd[3] + c]};
+    const float rp = st->rec[0][a.recd[0] + c];
+    // v stays in the stored scale (the transposed step is linear): the
+    // alpha cotangent is rescaled once, the output by out_scale / in_scale
+    float om = a.P.omega, omm = a.P.om;
+    if (a.omega_cell) om = omm = a.omega_cell[x];  // Tau::PerCell (BGK only)
+    float ab = collide_vjp<Q, COLL>(v, rp, u, st->alpha[c], a.P, om, omm) * a.in_scale_inv;
+    if constexpr (STG) {
+        if (a.stage) {
+            // the stage seed of this state: d(w . responses)/dg from its record
+            float Sm[6], fb[Q];
+#pragma unroll
+            for (int e = 0; e < 6; ++e) Sm[e] = st->rec[4 + e][a.recd[4 + e] + c];
+            const PortMap* pm = (m & MASK_PORT) ? &a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1] : nullptr;
+            ab += response_vjp<Q>(rp, u, Sm, st->alpha[c], pm ? pm->dp_weight : 0.f, pm != nullptr, a.seed,
+                                  a.P, fb);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) v[q] = fmaf(fb[q], s_in, v[q]);
+        }
+    }
+    a.abar[x] = fmaf(ab, a.abar_factor, ab_prev);
+    if (a.port_transpose && (m & MASK_PORT)) {
+        const PortMap& pm = a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1];
+        if (!pm.recon) {
+            port_transpose<Q>(pm, v);
+        } else {
+            // nonlinear ports, linearised at the recorded (rho, j / rho)
+            // of port_lin_cell (zero acceleration: u = j / (rho (1 +
+            // alpha / 2))); an extrapolating port's share for its
+            // neighbour stays in this cell's slots until the move that
+            // follows the step (launch_nee_move)
+            const size_t xm = (size_t)port_lin_cell(pm, x);
+            const float sc = 1.f + 0.5f * a.alpha[xm];
+            const float um[3] = {a.record[(size_t)n + xm] * sc, a.record[2 * (size_t)n + xm] * sc,
+                                 a.record[3 * (size_t)n + xm] * sc};
+            port_vjp<Q>(pm, a.record[xm], um, v);
+        }
+    }
+    store_own_lam<Q, T>(D, n, x, v, k_out);
+    if (a.norm2) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float sv = v[q] * k_out;
+            nsum += (double)sv * (double)sv;
+        }
+    }
+}
+
 // STG = 1: the stage-objective variant, which reads the second moments of
 // the recorded state as well and adds the state's response VJP.
 // LN = 2 (D3Q19, 16-bit storage, TRT/BGK or the folded bulk MRT, no stage
@@ -96,72 +166,6 @@ __global__ void __launch_bounds__(32 + 32 * (CONSUMER_WARPS / LN), (sizeof(T) ==
         uint32_t round = 0;
         const float s_in = 1.f / a.in_scale_inv;        // stored scale of the input
         const float k_out = a.out_scale * a.in_scale_inv;  // stored input -> stored output
-        // one cell c of the staged tile (mask m, the running alpha cotangent ab_prev)
-        auto one_cell = [&](const S* st, int c, uint32_t x, uint32_t m, float ab_prev) {
-            const bool fluid = !(m & MASK_SOLID);
-            if (!fluid) return;
-            float v[Q];
-            if (!(m & MASK_WRAP)) {
-#pragma unroll
-                for (int q = 0; q < Q; ++q)
-                    v[q] = Cvt<T>::to(st->run[q][(AL ? rund_aligned<Q, T, 1>(q) : a.rund[q]) + c]);
-                if (m & LINK_BITS) {
-                    // transposed bounce-back: the cell's own opposite slot
-#pragma unroll
-                    for (int q = 1; q < Q; ++q)
-                        if ((m >> opp<Q>(q)) & 1u) v[q] = Cvt<T>::to(B[opp<Q>(q) * n + x]);
-                }
-            } else {
-#pragma unroll
-                for (int q = 0; q < Q; ++q) v[q] = Cvt<T>::to(B[pull_adj_index<Q>(a.G, x, m, q)]);
-            }
-            const float u[3] = {st->rec[1][a.recd[1] + c], st->rec[2][a.recd[2] + c], st->rec[3][a.recd[3] + c]};
-            const float rp = st->rec[0][a.recd[0] + c];
-            // v stays in the stored scale (the transposed step is linear): the
-            // alpha cotangent is rescaled once, the output by out_scale / in_scale
-            float om = a.P.omega, omm = a.P.om;
-            if (a.omega_cell) om = omm = a.omega_cell[x];  // Tau::PerCell (BGK only)
-            float ab = collide_vjp<Q, COLL>(v, rp, u, st->alpha[c], a.P, om, omm) * a.in_scale_inv;
-            if constexpr (STG) {
-                if (a.stage) {
-                    // the stage seed of this state: d(w . responses)/dg from its record
-                    float Sm[6], fb[Q];
-#pragma unroll
-                    for (int e = 0; e < 6; ++e) Sm[e] = st->rec[4 + e][a.recd[4 + e] + c];
-                    const PortMap* pm = (m & MASK_PORT) ? &a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1] : nullptr;
-                    ab += response_vjp<Q>(rp, u, Sm, st->alpha[c], pm ? pm->dp_weight : 0.f, pm != nullptr, a.seed,
-                                          a.P, fb);
-#pragma unroll
-                    for (int q = 0; q < Q; ++q) v[q] = fmaf(fb[q], s_in, v[q]);
-                }
-            }
-            a.abar[x] = fmaf(ab, a.abar_factor, ab_prev);
-            if (a.port_transpose && (m & MASK_PORT)) {
-                const PortMap& pm = a.ports[((m >> MASK_PORT_SHIFT) & 7u) - 1];
-                if (!pm.recon) {
-                    port_transpose<Q>(pm, v);
-                } else {
-                    // nonlinear ports, linearised at the recorded (rho, j / rho)
-                    // of port_lin_cell (zero acceleration: u = j / (rho (1 +
-                    // alpha / 2))); an extrapolating port's share for its
-                    // neighbour stays in this cell's slots until the move that
-                    // follows the step (launch_nee_move)
-                    const size_t xm = (size_t)port_lin_cell(pm, x);
-                    const float sc = 1.f + 0.5f * a.alpha[xm];
-                    const float um[3] = {a.record[(size_t)n + xm] * sc, a.record[2 * (size_t)n + xm] * sc,
-                                         a.record[3 * (size_t)n + xm] * sc};
-                    port_vjp<Q>(pm, a.record[xm], um, v);
-                }
-            }
-            store_own_lam<Q, T>(D, n, x, v, k_out);
-            if (a.norm2) {
-#pragma unroll
-                for (int q = 0; q < Q; ++q) {
-                    const float sv = v[q] * k_out;
-                    nsum += (double)sv * (double)sv;
-                }
-            }
-        };
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
             if constexpr (LN == 1) {
                 const uint32_t x = tile * TILE + c0;
@@ -170,7 +174,8 @@ __global__ void __launch_bounds__(32 + 32 * (CONSUMER_WARPS / LN), (sizeof(T) ==
                 const float ab_prev = (!a.overwrite_abar && x < n) ? a.abar[x] : 0.f;
                 const bool ok = mbar_wait(&full[s], round & 1u, a.err);
                 const S* st = stage_at<S>(smem, s);
-                one_cell(st, c0, x, ok && x < n ? st->mask[c0] : MASK_SOLID, ab_prev);
+                adj_one_cell<Q, COLL, T, AL, STG>(a, st, c0, x, ok && x < n ? st->mask[c0] : MASK_SOLID, ab_prev, B, D, n,
+                                                  s_in, k_out, nsum);
             } else {
                 const int cA = c0, cB = c0 + 32 * CW;
                 const uint32_t xA = tile * TILE + cA, xB = tile * TILE + cB;
@@ -180,47 +185,48 @@ __global__ void __launch_bounds__(32 + 32 * (CONSUMER_WARPS / LN), (sizeof(T) ==
                 const S* st = stage_at<S>(smem, s);
                 const uint32_t mA = ok && xA < n ? st->mask[cA] : MASK_SOLID;
                 const uint32_t mB = ok && xB < n ? st->mask[cB] : MASK_SOLID;
-                if constexpr (COLL != CK_MRT && !STG) {
-                    if (!((mA | mB) & (MASK_SOLID | MASK_WRAP | MASK_PORT)) && !a.omega_cell) {
-                        F2 v[Q];
+                bool fast = false;
+                if constexpr (COLL != CK_MRT && !STG)
+                    fast = !((mA | mB) & (MASK_SOLID | MASK_WRAP | MASK_PORT)) && !a.omega_cell;
+                if (fast) {
+                    F2 v[Q];
 #pragma unroll
-                        for (int q = 0; q < Q; ++q) {
-                            const int off = AL ? rund_aligned<Q, T, 1>(q) : a.rund[q];
-                            v[q] = {make_float2(Cvt<T>::to(st->run[q][off + cA]), Cvt<T>::to(st->run[q][off + cB]))};
+                    for (int q = 0; q < Q; ++q) {
+                        const int off = AL ? rund_aligned<Q, T, 1>(q) : a.rund[q];
+                        v[q] = {make_float2(Cvt<T>::to(st->run[q][off + cA]), Cvt<T>::to(st->run[q][off + cB]))};
+                    }
+                    if ((mA | mB) & LINK_BITS) {
+#pragma unroll
+                        for (int q = 1; q < Q; ++q) {
+                            if ((mA >> opp<Q>(q)) & 1u) v[q].v.x = Cvt<T>::to(B[opp<Q>(q) * n + xA]);
+                            if ((mB >> opp<Q>(q)) & 1u) v[q].v.y = Cvt<T>::to(B[opp<Q>(q) * n + xB]);
                         }
-                        if ((mA | mB) & LINK_BITS) {
+                    }
+                    F2 u[3];
 #pragma unroll
-                            for (int q = 1; q < Q; ++q) {
-                                if ((mA >> opp<Q>(q)) & 1u) v[q].v.x = Cvt<T>::to(B[opp<Q>(q) * n + xA]);
-                                if ((mB >> opp<Q>(q)) & 1u) v[q].v.y = Cvt<T>::to(B[opp<Q>(q) * n + xB]);
-                            }
-                        }
-                        F2 u[3];
+                    for (int d = 0; d < 3; ++d)
+                        u[d] = {make_float2(st->rec[1 + d][a.recd[1 + d] + cA], st->rec[1 + d][a.recd[1 + d] + cB])};
+                    const F2 rp = {make_float2(st->rec[0][a.recd[0] + cA], st->rec[0][a.recd[0] + cB])};
+                    const F2 al = {make_float2(st->alpha[cA], st->alpha[cB])};
+                    const F2 ab = collide_vjp_lanes<Q, COLL, F2>(v, rp, u, al, a.P, a.P.omega, a.P.om, k_out);
+                    a.abar[xA] = fmaf(ab.v.x * a.in_scale_inv, a.abar_factor, pA);
+                    a.abar[xB] = fmaf(ab.v.y * a.in_scale_inv, a.abar_factor, pB);
 #pragma unroll
-                        for (int d = 0; d < 3; ++d)
-                            u[d] = {make_float2(st->rec[1 + d][a.recd[1 + d] + cA], st->rec[1 + d][a.recd[1 + d] + cB])};
-                        const F2 rp = {make_float2(st->rec[0][a.recd[0] + cA], st->rec[0][a.recd[0] + cB])};
-                        const F2 al = {make_float2(st->alpha[cA], st->alpha[cB])};
-                        const F2 ab = collide_vjp_lanes<Q, COLL, F2>(v, rp, u, al, a.P, a.P.omega, a.P.om, k_out);
-                        a.abar[xA] = fmaf(ab.v.x * a.in_scale_inv, a.abar_factor, pA);
-                        a.abar[xB] = fmaf(ab.v.y * a.in_scale_inv, a.abar_factor, pB);
+                    for (int q = 0; q < Q; ++q) {
+                        D[q * n + xA] = Cvt<T>::from(v[q].v.x);
+                        D[q * n + xB] = Cvt<T>::from(v[q].v.y);
+                    }
+                    if (a.norm2) {
 #pragma unroll
-                        for (int q = 0; q < Q; ++q) {
-                            D[q * n + xA] = Cvt<T>::from(v[q].v.x);
-                            D[q * n + xB] = Cvt<T>::from(v[q].v.y);
-                        }
-                        if (a.norm2) {
-#pragma unroll
-                            for (int q = 0; q < Q; ++q)
-                                nsum += (double)v[q].v.x * (double)v[q].v.x + (double)v[q].v.y * (double)v[q].v.y;
-                        }
-                    } else {
-                        one_cell(st, cA, xA, mA, pA);
-                        one_cell(st, cB, xB, mB, pB);
+                        for (int q = 0; q < Q; ++q)
+                            nsum += (double)v[q].v.x * (double)v[q].v.x + (double)v[q].v.y * (double)v[q].v.y;
                     }
                 } else {
-                    one_cell(st, cA, xA, mA, pA);
-                    one_cell(st, cB, xB, mB, pB);
+                    // the general path, one cell after the other (one inlined copy)
+#pragma unroll 1
+                    for (int h = 0; h < 2; ++h)
+                        adj_one_cell<Q, COLL, T, AL, STG>(a, st, h ? cB : cA, h ? xB : xA, h ? mB : mA, h ? pB : pA, B, D,
+                                                          n, s_in, k_out, nsum);
                 }
             }
             __syncwarp();
