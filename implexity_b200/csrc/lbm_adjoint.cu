@@ -11,7 +11,6 @@
 // the cell's own slots of the other array.  Loads are staged like the
 // forward step (lbm_device.cuh).
 #include "lbm_device.cuh"
-#include "lbm_vec2.cuh"
 
 namespace lbm {
 namespace {
@@ -49,10 +48,13 @@ __device__ __forceinline__ void adj_one_cell(const AdjArgs& a, const S* st, int 
     const float u[3] = {st->rec[1][a.recd[1] + c], st->rec[2][a.recd[2] + c], st->rec[3][a.recd[3] + c]};
     const float rp = st->rec[0][a.recd[0] + c];
     // v stays in the stored scale (the transposed step is linear): the
-    // alpha cotangent is rescaled once, the output by out_scale / in_scale
+    // alpha cotangent is rescaled once, the output by out_scale / in_scale --
+    // inside the collision transpose, unless a stage seed or a port transpose
+    // still acts on v before it is stored
     float om = a.P.omega, omm = a.P.om;
     if (a.omega_cell) om = omm = a.omega_cell[x];  // Tau::PerCell (BGK only)
-    float ab = collide_vjp<Q, COLL>(v, rp, u, st->alpha[c], a.P, om, omm) * a.in_scale_inv;
+    const bool post = (STG && a.stage) || (a.port_transpose && (m & MASK_PORT));
+    float ab = collide_vjp<Q, COLL>(v, rp, u, st->alpha[c], a.P, om, omm, post ? 1.f : k_out) * a.in_scale_inv;
     if constexpr (STG) {
         if (a.stage) {
             // the stage seed of this state: d(w . responses)/dg from its record
@@ -84,31 +86,24 @@ __device__ __forceinline__ void adj_one_cell(const AdjArgs& a, const S* st, int 
             port_vjp<Q>(pm, a.record[xm], um, v);
         }
     }
-    store_own_lam<Q, T>(D, n, x, v, k_out);
+    if (post) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) v[q] *= k_out;
+    }
+    store_own_lam<Q, T>(D, n, x, v, 1.f);
     if (a.norm2) {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const float sv = v[q] * k_out;
-            nsum += (double)sv * (double)sv;
-        }
+        for (int q = 0; q < Q; ++q) nsum += (double)v[q] * (double)v[q];
     }
 }
 
 // STG = 1: the stage-objective variant, which reads the second moments of
 // the recorded state as well and adds the state's response VJP.
-// LN = 2 (D3Q19, 16-bit storage, TRT/BGK or the folded bulk MRT, no stage
-// seeds): four consumer warps whose threads take two cells each, c and
-// c + 128 of the tile, and run the collision transpose for both at once in
-// packed FP32 pairs (collide_vjp_lanes, lbm_vec2.cuh); cells that need the
-// general path (solid, periodic face, port, per-cell tau) take the one-lane
-// body one after the other.  The 16-bit step is bound by instruction issue,
-// and the packed pairs halve its arithmetic.
-// Residency: three blocks per SM for 16-bit D3Q19 (LN = 1: 72 registers;
-// LN = 2: 160 threads with up to 136 registers); the others keep two blocks.
-template <int Q, int COLL, typename T, int AL, int STG, int LN>
-__global__ void __launch_bounds__(32 + 32 * (CONSUMER_WARPS / LN), (sizeof(T) == 2 && Q == 19 ? 3 : 2))
-    k_adjoint(AdjArgs a) {
-    constexpr int CW = CONSUMER_WARPS / LN;  // consumer warps
+// Residency: D3Q19 with 16-bit storage runs three blocks per SM (72
+// registers): its step is bound by latency and instruction issue, not bytes,
+// and a third block's warps hide more of it; the others keep two blocks.
+template <int Q, int COLL, typename T, int AL, int STG>
+__global__ void __launch_bounds__(TPB, (sizeof(T) == 2 && Q == 19 ? 3 : 2)) k_adjoint(AdjArgs a) {
     constexpr int NREC = STG ? 10 : 4;
     using S = AdjStage<Q, T, NREC>;
     constexpr int NCOPY = Q + NREC + 2;  // runs of lambda, the record, mask and alpha
@@ -126,7 +121,7 @@ __global__ void __launch_bounds__(32 + 32 * (CONSUMER_WARPS / LN), (sizeof(T) ==
 #pragma unroll
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], CW);
+            mbar_init(&empty[s], CONSUMER_WARPS);
         }
         mbar_fence_init();
     }
@@ -167,68 +162,14 @@ __global__ void __launch_bounds__(32 + 32 * (CONSUMER_WARPS / LN), (sizeof(T) ==
         const float s_in = 1.f / a.in_scale_inv;        // stored scale of the input
         const float k_out = a.out_scale * a.in_scale_inv;  // stored input -> stored output
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-            if constexpr (LN == 1) {
-                const uint32_t x = tile * TILE + c0;
-                // the running alpha cotangent, read before the wait so that its
-                // latency hides behind the staged copies and the collision
-                const float ab_prev = (!a.overwrite_abar && x < n) ? a.abar[x] : 0.f;
-                const bool ok = mbar_wait(&full[s], round & 1u, a.err);
-                const S* st = stage_at<S>(smem, s);
-                adj_one_cell<Q, COLL, T, AL, STG>(a, st, c0, x, ok && x < n ? st->mask[c0] : MASK_SOLID, ab_prev, B, D, n,
-                                                  s_in, k_out, nsum);
-            } else {
-                const int cA = c0, cB = c0 + 32 * CW;
-                const uint32_t xA = tile * TILE + cA, xB = tile * TILE + cB;
-                const float pA = (!a.overwrite_abar && xA < n) ? a.abar[xA] : 0.f;
-                const float pB = (!a.overwrite_abar && xB < n) ? a.abar[xB] : 0.f;
-                const bool ok = mbar_wait(&full[s], round & 1u, a.err);
-                const S* st = stage_at<S>(smem, s);
-                const uint32_t mA = ok && xA < n ? st->mask[cA] : MASK_SOLID;
-                const uint32_t mB = ok && xB < n ? st->mask[cB] : MASK_SOLID;
-                bool fast = false;
-                if constexpr (COLL != CK_MRT && !STG)
-                    fast = !((mA | mB) & (MASK_SOLID | MASK_WRAP | MASK_PORT)) && !a.omega_cell;
-                if (fast) {
-                    F2 v[Q];
-#pragma unroll
-                    for (int q = 0; q < Q; ++q) {
-                        const int off = AL ? rund_aligned<Q, T, 1>(q) : a.rund[q];
-                        v[q] = {make_float2(Cvt<T>::to(st->run[q][off + cA]), Cvt<T>::to(st->run[q][off + cB]))};
-                    }
-                    if ((mA | mB) & LINK_BITS) {
-#pragma unroll
-                        for (int q = 1; q < Q; ++q) {
-                            if ((mA >> opp<Q>(q)) & 1u) v[q].v.x = Cvt<T>::to(B[opp<Q>(q) * n + xA]);
-                            if ((mB >> opp<Q>(q)) & 1u) v[q].v.y = Cvt<T>::to(B[opp<Q>(q) * n + xB]);
-                        }
-                    }
-                    F2 u[3];
-#pragma unroll
-                    for (int d = 0; d < 3; ++d)
-                        u[d] = {make_float2(st->rec[1 + d][a.recd[1 + d] + cA], st->rec[1 + d][a.recd[1 + d] + cB])};
-                    const F2 rp = {make_float2(st->rec[0][a.recd[0] + cA], st->rec[0][a.recd[0] + cB])};
-                    const F2 al = {make_float2(st->alpha[cA], st->alpha[cB])};
-                    const F2 ab = collide_vjp_lanes<Q, COLL, F2>(v, rp, u, al, a.P, a.P.omega, a.P.om, k_out);
-                    a.abar[xA] = fmaf(ab.v.x * a.in_scale_inv, a.abar_factor, pA);
-                    a.abar[xB] = fmaf(ab.v.y * a.in_scale_inv, a.abar_factor, pB);
-#pragma unroll
-                    for (int q = 0; q < Q; ++q) {
-                        D[q * n + xA] = Cvt<T>::from(v[q].v.x);
-                        D[q * n + xB] = Cvt<T>::from(v[q].v.y);
-                    }
-                    if (a.norm2) {
-#pragma unroll
-                        for (int q = 0; q < Q; ++q)
-                            nsum += (double)v[q].v.x * (double)v[q].v.x + (double)v[q].v.y * (double)v[q].v.y;
-                    }
-                } else {
-                    // the general path, one cell after the other (one inlined copy)
-#pragma unroll 1
-                    for (int h = 0; h < 2; ++h)
-                        adj_one_cell<Q, COLL, T, AL, STG>(a, st, h ? cB : cA, h ? xB : xA, h ? mB : mA, h ? pB : pA, B, D,
-                                                          n, s_in, k_out, nsum);
-                }
-            }
+            const uint32_t x = tile * TILE + c0;
+            // the running alpha cotangent, read before the wait so that its
+            // latency hides behind the staged copies and the collision
+            const float ab_prev = (!a.overwrite_abar && x < n) ? a.abar[x] : 0.f;
+            const bool ok = mbar_wait(&full[s], round & 1u, a.err);
+            const S* st = stage_at<S>(smem, s);
+            adj_one_cell<Q, COLL, T, AL, STG>(a, st, c0, x, ok && x < n ? st->mask[c0] : MASK_SOLID, ab_prev, B, D, n,
+                                              s_in, k_out, nsum);
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);
             if (++s == STAGES) {
@@ -245,27 +186,18 @@ __global__ void __launch_bounds__(32 + 32 * (CONSUMER_WARPS / LN), (sizeof(T) ==
     }
 }
 
-template <int Q, int COLL, typename T, int AL, int STG, int LN>
+template <int Q, int COLL, typename T, int AL, int STG>
 cudaError_t run_adjoint_al(const AdjArgs& a, cudaStream_t s) {
     constexpr size_t smem = pipe_bytes<AdjStage<Q, T, STG ? 10 : 4>, ring_depth<AdjStage<Q, T, STG ? 10 : 4>, T>()>();
-    constexpr int threads = 32 + 32 * (CONSUMER_WARPS / LN);
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = set_smem(k_adjoint<Q, COLL, T, AL, STG, LN>, smem);
+        cudaError_t e = set_smem(k_adjoint<Q, COLL, T, AL, STG>, smem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    const int grid = persistent_grid((const void*)k_adjoint<Q, COLL, T, AL, STG, LN>, a.G.n, smem, threads, TILE);
-    k_adjoint<Q, COLL, T, AL, STG, LN><<<grid, threads, smem, s>>>(a);
+    const int grid = persistent_grid((const void*)k_adjoint<Q, COLL, T, AL, STG>, a.G.n, smem, TPB, TILE);
+    k_adjoint<Q, COLL, T, AL, STG><<<grid, TPB, smem, s>>>(a);
     return cudaGetLastError();
-}
-
-// The two-lane consumers (LN = 2) serve D3Q19 with 16-bit storage, no stage
-// seeds and a collision other than the general MRT.
-template <int Q, int COLL, typename T, int AL, int STG>
-cudaError_t run_adjoint_ln(const AdjArgs& a, cudaStream_t s) {
-    if constexpr (Q == 19 && sizeof(T) == 2 && COLL != CK_MRT && !STG) return run_adjoint_al<Q, COLL, T, AL, STG, 2>(a, s);
-    else return run_adjoint_al<Q, COLL, T, AL, STG, 1>(a, s);
 }
 
 template <int Q, typename T>
@@ -281,8 +213,8 @@ template <int Q, int COLL, typename T>
 cudaError_t run_adjoint(const AdjArgs& a, cudaStream_t s) {
     const bool al = adj_table_is_aligned<Q, T>(a.rund);
     if (a.rec_planes == 10)
-        return al ? run_adjoint_ln<Q, COLL, T, 1, 1>(a, s) : run_adjoint_ln<Q, COLL, T, 0, 1>(a, s);
-    return al ? run_adjoint_ln<Q, COLL, T, 1, 0>(a, s) : run_adjoint_ln<Q, COLL, T, 0, 0>(a, s);
+        return al ? run_adjoint_al<Q, COLL, T, 1, 1>(a, s) : run_adjoint_al<Q, COLL, T, 0, 1>(a, s);
+    return al ? run_adjoint_al<Q, COLL, T, 1, 0>(a, s) : run_adjoint_al<Q, COLL, T, 0, 0>(a, s);
 }
 
 }  // namespace

@@ -873,7 +873,7 @@ __device__ __forceinline__ Macro collide_fused_dp(float (&vf)[Q], float alpha_f,
 // Brinkman chain F = rho (a - alpha u), u = (m/rho + a/2)/(1 + alpha/2).
 template <int Q, int COLL>
 __device__ __forceinline__ float collide_vjp(float (&gb)[Q], float rp, const float (&u)[3], float alpha,
-                                             const Physics& P, float om, float omm) {
+                                             const Physics& P, float om, float omm, float k = 1.f) {
     using L = Lat<Q>;
     constexpr int NP = L::NPAIR;
     const float rho = 1.f + rp;
@@ -1004,34 +1004,51 @@ __device__ __forceinline__ float collide_vjp(float (&gb)[Q], float rp, const flo
         sbar -= ub[d] * u[d] * inv_s;
     }
     abar += 0.5f * sbar;
-    // output: gb - R^T gb + rho_bar + c . mb, pair by pair (with the MRT
-    // corrections, which are even: the same for i and opp(i))
-    const float hp = 0.5f * (1.f - om), hm = 0.5f * (1.f - omm);
-    gb[0] = g0 + rho_bar;
+    // output, times k: gb - R^T gb + rho_bar + c . mb, pair by pair (with
+    // the MRT corrections, which are even: the same for i and opp(i)); the
+    // scale k of the stored cotangent enters the few per-cell coefficients
+    // instead of every population
+    const float hp = 0.5f * (1.f - om) * k, hm = 0.5f * (1.f - omm) * k;
+    const float kr = k * rho_bar, kbulk = k * bulk_c;
+    float kmb[3];
 #pragma unroll
-    for (int k = 0; k < NP; ++k) {
-        const int i = k + 1, o = opp<Q>(i);
-        float base = rho_bar;
+    for (int d = 0; d < 3; ++d) kmb[d] = k * mb[d];
+    gb[0] = fmaf(k, g0, kr);
+#pragma unroll
+    for (int kk = 0; kk < NP; ++kk) {
+        const int i = kk + 1, o = opp<Q>(i);
+        float base = kr;
         if constexpr (COLL == CK_MRT_BULK) {
             const int c2 = L::cx(i) * L::cx(i) + L::cy(i) * L::cy(i) + L::cz(i) * L::cz(i);
-            if (c2 != 1) base = fmaf(-bulk_c, (float)(c2 - 1), base);  // folded after unrolling
+            if (c2 != 1) base = fmaf(-kbulk, (float)(c2 - 1), base);  // folded after unrolling
         }
-        float pi = fmaf(hp, SM[k], base), po = pi;
+        float pi = fmaf(hp, SM[kk], base), po = pi;
         if constexpr (COLL == CK_MRT) {
 #pragma unroll
             for (int p = 0; p < MAX_PROJ; ++p)
                 if (p < P.n_proj) {
-                    pi = fmaf(-cproj[p], P.proj_right[p][i], pi);
-                    po = fmaf(-cproj[p], P.proj_right[p][o], po);
+                    pi = fmaf(-k * cproj[p], P.proj_right[p][i], pi);
+                    po = fmaf(-k * cproj[p], P.proj_right[p][o], po);
                 }
         }
-        float cm = 0.f;
-        if (L::cx(i)) cm = fmaf((float)L::cx(i), mb[0], cm);
-        if (L::cy(i)) cm = fmaf((float)L::cy(i), mb[1], cm);
-        if (L::cz(i)) cm = fmaf((float)L::cz(i), mb[2], cm);
-        const float d = fmaf(hm, DF[k], cm);
-        gb[i] = pi + d;
-        gb[o] = po - d;
+        // c . kmb accumulated from the first nonzero component of the
+        // direction whose first component is positive (no negations)
+        const int c[3] = {L::cx(i), L::cy(i), L::cz(i)};
+        const int first = c[0] ? 0 : (c[1] ? 1 : 2);
+        const int sg = c[first] > 0 ? 1 : -1;
+        float cm = kmb[first];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (d != first && c[d]) cm = sg * c[d] > 0 ? cm + kmb[d] : cm - kmb[d];
+        if (sg > 0) {
+            const float d = fmaf(hm, DF[kk], cm);  // hm DF + c . mb
+            gb[i] = pi + d;
+            gb[o] = po - d;
+        } else {
+            const float d = fmaf(-hm, DF[kk], cm);  // -(hm DF + c . mb)
+            gb[i] = pi - d;
+            gb[o] = po + d;
+        }
     }
     return abar;
 }
