@@ -179,3 +179,34 @@ def test_extrapolating_ports_steady_gradient_matches_oracle(gpu_lib):
         g, rep = s.gradient(w, mode="steady", tolerance=1e-10)
     assert rep.converged
     assert _rel_l2(g, g_ref) < 1e-4, _rel_l2(g, g_ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("inlet,outlet", [("non_equilibrium_extrapolation", "neighbor_non_equilibrium"),
+                                          ("regularized_known_stress", "regularized_known_stress")])
+def test_nonlinear_ports_with_16_bit_storage(gpu_lib, inlet, outlet):
+    """The 16-bit stepping path ((f - w)/w storage units) through the same
+    ports, against the FP64 oracle at the 16-bit bars: velocity 2e-3 of its
+    largest value, horizon gradient 1e-3 relative L2."""
+    norm = normalize(nee_channel(inlet, outlet, storage="float16"))
+    raw = workloads.uniform_design(norm.shape, 4)
+    w = workloads.objective_weights()
+    o = Oracle(norm)
+    phi_r, alpha_r = o.design(raw)
+    f_r, d_r = o.history(alpha_r, norm.step_count)
+    g_h, _, _, st = o.gradient(raw, w, mode="horizon", K=20)
+    assert st == 0
+    from test_gpu_parity import macroscopic
+
+    with LbmSolver(norm) as s:
+        s.set_design(raw)
+        d = s.forward()
+        assert d.admitted
+        f = s.populations()
+        g, _ = s.gradient(w, mode="horizon", checkpoint_every=20)
+    fluid = ~np.asarray(norm.solid_mask, bool).reshape(-1)
+    a = np.asarray(o.acceleration_lattice)
+    _, u = macroscopic(f[fluid], o.q, alpha_r[fluid], a)
+    _, u_r = macroscopic(f_r[fluid], o.q, alpha_r[fluid], a)
+    assert float(np.max(np.abs(u - u_r)) / np.max(np.abs(u_r))) < 2e-3
+    assert _rel_l2(g, g_h) < 1e-3, _rel_l2(g, g_h)
