@@ -117,6 +117,22 @@ def test_regularized_port_keeps_the_legacy_density_and_velocity():
         assert np.max(np.abs(reg - leg)) > 1e-6  # the known populations are rebuilt too
 
 
+def test_slab_handles_take_legacy_ports_only():
+    import ctypes as C
+
+    from implexity_b200 import ContractError, _abi
+    from implexity_b200.solver import _raise
+
+    norm = normalize(nee_channel("legacy_moment", "neighbor_non_equilibrium"))
+    lib = _abi.load()
+    cp = norm.to_c()
+    h = C.c_void_p()
+    st = lib.lbm_create_slab(C.byref(cp), 0, norm.shape[0] // 2, 1, C.byref(h))
+    assert st != _abi.LBM_OK
+    with pytest.raises(ContractError, match="legacy_moment ports only"):
+        _raise(st, lib.lbm_last_error(None).decode())
+
+
 def _create(prob):
     """lbm_create's validation only (no device needed when it refuses)."""
     import ctypes as C
